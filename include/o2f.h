@@ -1,0 +1,250 @@
+/*
+ * o2f.h -- C ABI of the B200 implementation of the shape-gradient hot path of
+ * the 2-D compressible Navier-Stokes adjoint shape optimiser
+ * (ThibaultMaurelOujia/Optimisation2Forme).
+ *
+ * The reference has no FFI layer: its path is a set of C++ free functions in
+ * namespace navier_stokes that mutate an array-of-structs Mesh&.  Each entry
+ * point below replaces one of them (reference file:line in its comment).  The
+ * device-resident solver context plays the role of the reference Mesh: it owns
+ * the renumbered mesh, the cell state, the interface states and wall stresses
+ * left by the last residual, and all scratch memory.
+ *
+ * Conventions
+ *  - Every function returns O2F_OK (0) or a negative o2f_status; no exception
+ *    crosses the ABI.  o2f_last_error() returns a message for the calling
+ *    thread's last failure.
+ *  - Arrays at the boundary are in the REFERENCE orders (cells in Gmsh element
+ *    order, edges in (vmin,vmax) lexicographic order), interleaved 4*i+k for
+ *    per-cell 4-vectors (rho, rho_u, rho_v, E) exactly like the reference's
+ *    adjoint vectors (src/shape_optimization.cpp:616-629).  Internally the
+ *    mesh is renumbered along a Hilbert curve; that permutation never leaks.
+ *  - Pointers passed with a *_host suffix are host memory; *_dev pointers are
+ *    device memory on the context's device.  All work is issued on the
+ *    context's stream; functions that return host values synchronise it.
+ *  - One context per host thread at a time (like the reference, which is not
+ *    reentrant); several contexts may coexist in one process, unlike the
+ *    reference whose function-static scratch buffers tie a process to one
+ *    mesh size (src/advection.cpp:9-23).
+ */
+#ifndef O2F_H
+#define O2F_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum o2f_status {
+  O2F_OK = 0,
+  O2F_ERR_ARG = -1,        /* invalid argument (null pointer, bad size)       */
+  O2F_ERR_IO = -2,         /* file cannot be opened / parsed                  */
+  O2F_ERR_MESH = -3,       /* mesh topology unsupported or inconsistent       */
+  O2F_ERR_CUDA = -4,       /* CUDA runtime error                              */
+  O2F_ERR_NONFINITE = -5,  /* NaN/Inf in a state, residual or Krylov scalar   */
+  O2F_ERR_NOT_CONVERGED = -6, /* iteration cap reached before tolerance      */
+  O2F_ERR_BREAKDOWN = -7,  /* BiCGSTAB breakdown (rho or omega ~ 0)          */
+  O2F_ERR_STATE = -8       /* call order violated (e.g. adjoint before a residual) */
+} o2f_status;
+
+/* Boundary codes, identical to the reference's char codes
+ * (src/mesh.cpp:84-108, src/boundary.cpp:19-42). */
+#define O2F_BC_NONE 0
+#define O2F_BC_INLET 'i'
+#define O2F_BC_OUTLET 'o'
+#define O2F_BC_FARFIELD 'f'
+#define O2F_BC_WALL 'w'
+
+/* Limiter choice.  VENKAT is the reference's live limiter
+ * (src/advection.cpp:209-230, eps=(k*h)^3); BARTH_JESPERSEN is the
+ * reference's commented-out alternative (src/advection.cpp:195-207). */
+#define O2F_LIMITER_VENKAT 0
+#define O2F_LIMITER_BARTH_JESPERSEN 1
+
+/* Arithmetic of the residual / Jacobian-transpose kernels. */
+#define O2F_PREC_F64 0 /* FP64 throughout (parity mode)                           */
+#define O2F_PREC_F32 1 /* FP32 residual and JT, FP64 reductions, dt and Krylov     */
+
+/* Physics and numerics.  Field names and defaults mirror the reference's
+ * SimulationParams (include/params.hpp:15-81) plus the keys the reference
+ * hard-codes (marked NEW).  o2f_params_default() fills the reference
+ * defaults after SimulationParams::finalize() (src/params.cpp:5-8). */
+typedef struct o2f_params {
+  double gamma;           /* 1.4                                              */
+  double viscosity;       /* dynamic viscosity mu [Pa s]                      */
+  double Pr;              /* Prandtl number                                    */
+  double cp;              /* 1005                                              */
+  double cfl_number;      /* CFL of the global time step                       */
+  double final_time;      /* time-loop end (src/simulation.cpp:75)             */
+  double inflow_velocity; /* freestream Mach number (src/boundary.cpp:12)      */
+  double rho_ref;         /* 1.225                                             */
+  double p_ref;           /* 101325                                            */
+  double aoa_deg;         /* NEW: angle of attack, rotates the freestream and
+                             the lift/drag axes; 0 reproduces the reference    */
+  double limiter_k;       /* NEW: Venkatakrishnan K, eps=(K h)^3; reference 1e-2 */
+  int limiter;            /* NEW: O2F_LIMITER_*                                */
+  int precision;          /* NEW: O2F_PREC_*                                   */
+} o2f_params;
+
+void o2f_params_default(o2f_params* p);
+
+/* Mesh description in the reference's construction order (src/mesh.cpp:7-283):
+ *  - nodes in vertex order (Gmsh node-tag order);
+ *  - boundary segments in physical-group order: a vertex touched by several
+ *    groups keeps the LAST code, as in the reference (src/mesh.cpp:84-108);
+ *  - cells (triangles: 3 vertices, quads: 4) in element order, counter- or
+ *    clockwise.  cell_offsets[n_cells] = total vertex count. */
+typedef struct o2f_mesh_desc {
+  int64_t n_nodes;
+  const double* node_xy;     /* [n_nodes*2]                                    */
+  int64_t n_segments;
+  const int64_t* segments;   /* [n_segments*2] vertex indices                  */
+  const uint8_t* segment_bc; /* [n_segments] O2F_BC_* codes                    */
+  int64_t n_cells;
+  const int64_t* cell_offsets; /* [n_cells+1]                                  */
+  const int64_t* cell_nodes;   /* vertex indices                               */
+} o2f_mesh_desc;
+
+typedef struct o2f_mesh_info {
+  int64_t n_cells, n_edges, n_vertices;
+  int64_t n_wall_edges, n_boundary_edges;
+  int64_t max_vertex_valence;
+  double min_h; /* min over cells of 2V/perimeter (src/simulation.cpp:98-104) */
+  size_t device_bytes;
+} o2f_mesh_info;
+
+typedef struct o2f_ctx o2f_ctx;
+typedef struct o2f_host_mesh o2f_host_mesh;
+
+const char* o2f_last_error(void);
+const char* o2f_version(void);
+
+/* Host-only mesh build (no GPU needed): the topology, geometry and
+ * interpolation weights the context is built from, in reference order.  The
+ * construction replaces navier_stokes::Mesh::Mesh (src/mesh.cpp:7-283) and
+ * recordEdge (:288-297).  Export names: see o2f_mesh_export. */
+int o2f_host_mesh_create(const o2f_mesh_desc* mesh, o2f_host_mesh** out);
+int o2f_host_mesh_from_msh(const char* path, o2f_host_mesh** out);
+int o2f_host_mesh_export(const o2f_host_mesh* mesh, const char* which, void* out, int64_t* count);
+int o2f_host_mesh_destroy(o2f_host_mesh* mesh);
+
+/* Build a context: replaces navier_stokes::Mesh::Mesh(params)
+ * (src/mesh.cpp:7-283; include/mesh.hpp:116) followed by the solver set-up.
+ * `stream` is a cudaStream_t (NULL: the context creates its own). */
+int o2f_create(const o2f_mesh_desc* mesh, const o2f_params* params, void* stream, o2f_ctx** out);
+/* Same, reading an ASCII MSH 2.2 file with physical groups named Inlet,
+ * Outlet, FreeStream, Wall or Airfoil, as the reference's Gmsh import does. */
+int o2f_create_from_msh(const char* path, const o2f_params* params, void* stream, o2f_ctx** out);
+int o2f_destroy(o2f_ctx* ctx);
+int o2f_set_params(o2f_ctx* ctx, const o2f_params* params);
+int o2f_get_info(const o2f_ctx* ctx, o2f_mesh_info* info);
+
+/* Topology and geometry in reference order, for checking the mesh build
+ * (integer arrays must equal the reference's exactly).  `which` selects one
+ * array; *count receives its length; pass out=NULL to query the length.
+ * Names: "edge_v","edge_c","edge_bc","cell_edges_off","cell_edges",
+ * "vert_cells_off","vert_cells","vert_cells_ord","cell_verts_off",
+ * "cell_verts","vert_bc" (int64) and "vert_xy","edge_len","edge_n",
+ * "edge_ctr","cell_vol","cell_ctr","vert_w" (double). */
+int o2f_mesh_export(const o2f_ctx* ctx, const char* which, void* out, int64_t* count);
+
+/* Cell state, [n_cells*4] interleaved, reference cell order.  Replaces
+ * loadCellStates / saveCellStates (src/utils.cpp:29-107) at the device
+ * boundary; the text format itself is handled by the host helpers. */
+int o2f_state_set(o2f_ctx* ctx, const double* U_host);
+int o2f_state_get(o2f_ctx* ctx, double* U_host);
+/* Uniform freestream, init_one_x (src/init.cpp:57-81), rotated by aoa. */
+int o2f_state_freestream(o2f_ctx* ctx);
+
+/* One residual evaluation: computeAdvectionTerm + computeDiffusionTerm
+ * (src/advection.cpp:415-466, src/diffusion.cpp:206-243), i.e.
+ * computeResidual (src/shape_optimization.cpp:171-189).  Leaves the interface
+ * states and wall stresses in the context (as the reference leaves them in
+ * Mesh::edges).  R_host may be NULL. */
+int o2f_residual(o2f_ctx* ctx, double* R_host);
+
+/* Per-stage arrays of the last residual, reference order:
+ * "grad" [n_cells*8] (rho_x,rho_u_x,rho_v_x,E_x,rho_y,...), "edge_LR"
+ * [n_edges*8], "edge_tau" [n_edges*3], "vertex_U" [n_vertices*4], "R". */
+int o2f_debug_get(o2f_ctx* ctx, const char* which, double* out_host);
+
+/* SSP-RK3 time loop, Simulator::time_loop (src/simulation.cpp:68-142):
+ * steps while t < final_time, at most max_steps steps, and (NEW) stops when
+ * ||R_rho||_2 has dropped by drop_tol relative to the first step (0: off).
+ * history_host (may be NULL) receives ||R_rho||_2 of each step's first stage,
+ * [max_steps]. */
+int o2f_rk3_run(o2f_ctx* ctx, int64_t max_steps, double drop_tol, double* history_host,
+                int64_t* steps_done, double* t_out);
+
+/* computeLiftDragCoefficients (src/compute.cpp:92-132) and
+ * computeDirectObjectiveTerm J = -C_L + beta*C_D
+ * (src/shape_optimization.cpp:893-939, wall edges with centre.x > 1.3
+ * skipped), from the interface states of the last residual.
+ * forces_out = {C_L, C_D, J}. */
+int o2f_forces(o2f_ctx* ctx, double beta, double* forces_out);
+
+/* y = J^T x, applyJacobianTranspose (src/shape_optimization.cpp:237-484),
+ * about the interface states of the last residual.  x, y [n_cells*4]. */
+int o2f_jt_apply(o2f_ctx* ctx, const double* x_host, double* y_host);
+
+/* b = dJ/dU, assembleAdjointRHS (src/shape_optimization.cpp:491-554). */
+int o2f_adjoint_rhs(o2f_ctx* ctx, double beta, double* b_host);
+
+/* Solve J^T lambda = b with restarted BiCGSTAB, solveAdjointSystem
+ * (src/shape_optimization.cpp:658-740): inner chunks of `restart`
+ * iterations, a true-residual check after each, stop at relres <= tol.
+ * lambda_host may be NULL (lambda stays in the context). */
+int o2f_adjoint_solve(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, int64_t restart,
+                      double* lambda_host, int64_t* iters, double* relres);
+
+/* NACA-4 shape parameters (src/shape_optimization.cpp:830-834 defaults). */
+typedef struct o2f_shape_params {
+  double pos_x; /* 0.355 */
+  double c;     /* 1.0   */
+  double m;     /* 0.02  */
+  double p;     /* 0.4   */
+  double t;     /* 0.12  */
+} o2f_shape_params;
+
+/* Gradient parameter selectors. */
+#define O2F_PARAM_M 0
+#define O2F_PARAM_P 1
+#define O2F_PARAM_T 2 /* NEW: the reference returns without perturbing for t */
+
+/* Shape gradient g_k = dJ_direct/dtheta_k - lambda . dR/dtheta_k by central
+ * differences, computeShapeGradient (src/shape_optimization.cpp:942-1016),
+ * with applyShapePerturbationNACA12 + updateDerivedGeometry (:748-890).
+ * lambda_host == NULL uses the context's last adjoint solution. */
+int o2f_shape_gradient(o2f_ctx* ctx, const o2f_shape_params* shape, const int* param_ids, int n_params,
+                       double beta, double eps, const double* lambda_host, double* grad_out);
+
+/* The whole of optimizeShape (src/shape_optimization.cpp:1022-1067):
+ * J from the current interface states, adjoint solve, shape gradient.
+ * out = {J, iters, relres}. */
+int o2f_optimize_shape(o2f_ctx* ctx, const o2f_shape_params* shape, const int* param_ids, int n_params,
+                       double beta, double eps, double tol, double* grad_out, double* out);
+
+/* Geometry after applyShapePerturbationNACA12(param, eps) for checking:
+ * "vert_xy","edge_len","edge_n","edge_ctr","cell_vol","cell_ctr","vert_w". */
+int o2f_debug_perturbed(o2f_ctx* ctx, const o2f_shape_params* shape, int param_id, double eps,
+                        const char* which, double* out_host);
+
+/* Device pointers (n_cells*4, interleaved, INTERNAL Hilbert order) and
+ * the permutation old->new, for device-resident callers. */
+int o2f_state_device(o2f_ctx* ctx, double** U_dev);
+int o2f_cell_permutation(const o2f_ctx* ctx, int64_t* new_of_old_host);
+
+/* Timing of the last o2f_rk3_run / o2f_adjoint_solve, per kernel class. */
+typedef struct o2f_timing {
+  double residual_ms;  /* last o2f_residual */
+  int64_t kernel_launches;
+} o2f_timing;
+int o2f_get_timing(const o2f_ctx* ctx, o2f_timing* t);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* O2F_H */

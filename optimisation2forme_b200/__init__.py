@@ -1,0 +1,13 @@
+"""B200 implementation of the shape-gradient hot path of a 2-D compressible
+Navier-Stokes adjoint shape optimiser (ThibaultMaurelOujia/Optimisation2Forme).
+
+The compute lives in the native library ``libo2f.so`` (C ABI in
+``include/o2f.h``, CUDA kernels for sm_100a); this package is the host-side
+binding.  Importing works without a GPU; creating a ``Solver`` needs one.
+"""
+from ._lib import LIB_PATH, O2FError, lib
+from .solver import (HostMesh, SimulationParams, Solver, load_cell_states, load_config, load_params_generic,
+                     mesh_desc, save_cell_states, write_shape_log)
+
+__all__ = ["LIB_PATH", "O2FError", "lib", "HostMesh", "SimulationParams", "Solver", "load_cell_states",
+           "load_config", "load_params_generic", "mesh_desc", "save_cell_states", "write_shape_log"]

@@ -1,0 +1,887 @@
+// Host drivers of the solver context: device upload of the renumbered mesh and
+// the launch sequences of the residual, time loop, adjoint and shape gradient.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "kernels_adjoint.cuh"
+
+namespace o2f {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(O2F_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DeviceArena::~DeviceArena() {
+  for (void* p : ptrs_) cudaFree(p);
+}
+
+void* DeviceArena::raw(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 32;
+  O2F_CUDA(cudaMalloc(&p, bytes));
+  ptrs_.push_back(p);
+  bytes_ += bytes;
+  return p;
+}
+
+namespace {
+
+template <typename X>
+void h2d(X* dst, const std::vector<X>& src, cudaStream_t s) {
+  if (!src.empty()) O2F_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(X), cudaMemcpyHostToDevice, s));
+}
+
+void validate_params(const o2f_params& p) {
+  if (!(p.gamma > 1.0) || !(p.viscosity > 0.0) || !(p.Pr > 0.0) || !(p.cp > 0.0) || !(p.rho_ref > 0.0) ||
+      !(p.p_ref > 0.0) || !(p.cfl_number > 0.0) || !(p.inflow_velocity >= 0.0) || !(p.limiter_k > 0.0))
+    throw Error(O2F_ERR_ARG, "invalid physical parameters");
+  if (p.limiter != O2F_LIMITER_VENKAT && p.limiter != O2F_LIMITER_BARTH_JESPERSEN)
+    throw Error(O2F_ERR_ARG, "unknown limiter");
+  if (p.precision != O2F_PREC_F64) throw Error(O2F_ERR_ARG, "this context supports O2F_PREC_F64");
+}
+
+}  // namespace
+
+Solver::Solver(const o2f_mesh_desc& desc, const o2f_params& p, cudaStream_t stream) {
+  validate_params(p);
+  try {
+    hm_ = build_mesh(desc);
+  } catch (const std::invalid_argument& e) {
+    throw Error(O2F_ERR_ARG, e.what());
+  } catch (const std::runtime_error& e) {
+    throw Error(O2F_ERR_MESH, e.what());
+  }
+  if (hm_.nc >= (int64_t(1) << 30) || hm_.ne >= (int64_t(1) << 30)) throw Error(O2F_ERR_MESH, "mesh too large");
+  int dev_count = 0;
+  O2F_CUDA(cudaGetDeviceCount(&dev_count));
+  if (stream) {
+    stream_ = stream;
+  } else {
+    O2F_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    own_stream_ = true;
+  }
+  O2F_CUDA(cudaEventCreate(&ev0_));
+  O2F_CUDA(cudaEventCreate(&ev1_));
+  params_ = p;
+  min_h_ = min_cell_h(hm_);
+  upload_mesh();
+  set_params(p);
+  state_freestream();
+  sync();
+}
+
+Solver::~Solver() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+}
+
+void Solver::sync() { O2F_CUDA(cudaStreamSynchronize(stream_)); }
+
+void Solver::compute_phys() {
+  const o2f_params& p = params_;
+  Phys ph{};
+  ph.gamma = p.gamma;
+  ph.mu = p.viscosity;
+  ph.cp = p.cp;
+  ph.Pr = p.Pr;
+  ph.kappa = p.viscosity * p.cp / p.Pr;  // src/diffusion.cpp:210
+  // Freestream (src/boundary.cpp:10-17), rotated by the angle of attack;
+  // cos(0) = 1 and sin(0) = 0 keep the reference's values bit for bit.
+  const double rho0 = p.rho_ref, p0 = p.p_ref, M = p.inflow_velocity;
+  const double a0 = std::sqrt(p.gamma * p0 / rho0);
+  const double u0 = M * a0;
+  const double alpha = p.aoa_deg * (3.14159265358979323846 / 180.0);
+  ph.cos_a = std::cos(alpha);
+  ph.sin_a = std::sin(alpha);
+  if (p.aoa_deg == 0.0) {
+    ph.cos_a = 1.0;
+    ph.sin_a = 0.0;
+  }
+  const double ux = u0 * ph.cos_a, uy = u0 * ph.sin_a;
+  const double kinetic = 0.5 * rho0 * (ux * ux + uy * uy);
+  ph.fs_rho = rho0;
+  ph.fs_rhou = rho0 * ux;
+  ph.fs_rhov = rho0 * uy;
+  ph.fs_E = p.p_ref / (p.gamma - 1.0) + kinetic;
+  // q_inf of computeLiftDragCoefficients (src/compute.cpp:93-100).
+  const double a_inf = std::sqrt(p.gamma * p0 / rho0);
+  const double U_inf = M * a_inf;
+  ph.q_inf = 0.5 * (rho0 * U_inf * U_inf);
+  ph.limiter_k = p.limiter_k;
+  ph.limiter = p.limiter;
+  phys_ = ph;
+}
+
+void Solver::set_params(const o2f_params& p) {
+  validate_params(p);
+  params_ = p;
+  compute_phys();
+  k_venkat_eps<double><<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, p.limiter_k, geom_.cgeom);
+  O2F_CUDA(cudaGetLastError());
+  blk_valid_ = false;
+}
+
+void Solver::upload_mesh() {
+  const HostMesh& m = hm_;
+  const int64_t nc = m.nc, ne = m.ne, nv = m.nv;
+  // Hilbert order of cells and vertices; edges follow their lower-numbered cell.
+  cperm_ = hilbert_order(m.ccx, m.ccy);
+  vperm_ = hilbert_order(m.vx, m.vy);
+  cinv_.assign(nc, 0);
+  vinv_.assign(nv, 0);
+  for (int64_t i = 0; i < nc; ++i) cinv_[cperm_[i]] = i;
+  for (int64_t i = 0; i < nv; ++i) vinv_[vperm_[i]] = i;
+  std::vector<int64_t> ekey(ne);
+  for (int64_t e = 0; e < ne; ++e) {
+    int64_t a = cinv_[m.e_cl[e]];
+    int64_t b = m.e_cr[e] >= 0 ? cinv_[m.e_cr[e]] : a;
+    ekey[e] = std::min(a, b);
+  }
+  eperm_.resize(ne);
+  std::iota(eperm_.begin(), eperm_.end(), 0);
+  std::stable_sort(eperm_.begin(), eperm_.end(), [&](int64_t x, int64_t y) { return ekey[x] < ekey[y]; });
+  einv_.assign(ne, 0);
+  for (int64_t i = 0; i < ne; ++i) einv_[eperm_[i]] = i;
+
+  topo_.nc = nc;
+  topo_.ne = ne;
+  topo_.nv = nv;
+  topo_.nnz = (int64_t)m.vert_wcells.size();
+
+  // Cells.
+  std::vector<int32_t> slot(4 * nc, -1), jslot(4 * nc, -1), cverts(4 * nc, -1);
+  std::vector<uint8_t> ctype(nc);
+  std::vector<Vec4<double>> cgeom(nc);
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t co = cperm_[c];
+    const int64_t o0 = m.cell_eoff[co], o1 = m.cell_eoff[co + 1];
+    std::vector<int64_t> ids(m.cell_edges.begin() + o0, m.cell_edges.begin() + o1);
+    for (int64_t k = 0; k < o1 - o0; ++k) {
+      const int64_t eo = ids[k];
+      const int side = (m.e_cl[eo] == co) ? 0 : 1;
+      slot[k * nc + c] = (int32_t)(2 * einv_[eo] + side);
+    }
+    std::sort(ids.begin(), ids.end());
+    for (int64_t k = 0; k < o1 - o0; ++k) {
+      const int64_t eo = ids[k];
+      const int side = (m.e_cl[eo] == co) ? 0 : 1;
+      jslot[k * nc + c] = (int32_t)(2 * einv_[eo] + side);
+    }
+    const int64_t v0 = m.cell_voff[co], v1 = m.cell_voff[co + 1];
+    ctype[c] = (uint8_t)(v1 - v0);
+    for (int64_t k = 0; k < v1 - v0; ++k) cverts[4 * c + k] = (int32_t)vinv_[m.cell_verts[v0 + k]];
+    cgeom[c] = Vec4<double>{m.ccx[co], m.ccy[co], m.cvol[co], 0.0};
+  }
+  // Edges.
+  std::vector<int2> ev(ne), ec(ne);
+  std::vector<uint8_t> ebc(ne);
+  std::vector<Vec4<double>> egeom(ne);
+  std::vector<Vec2<double>> ectr(ne);
+  for (int64_t e = 0; e < ne; ++e) {
+    const int64_t eo = eperm_[e];
+    ev[e] = make_int2((int)vinv_[m.e_v0[eo]], (int)vinv_[m.e_v1[eo]]);
+    ec[e] = make_int2((int)cinv_[m.e_cl[eo]], m.e_cr[eo] >= 0 ? (int)cinv_[m.e_cr[eo]] : -1);
+    ebc[e] = m.ebc[eo];
+    egeom[e] = Vec4<double>{m.enx[eo], m.eny[eo], m.elen[eo], 0.0};
+    ectr[e] = Vec2<double>{m.ecx[eo], m.ecy[eo]};
+  }
+  // Vertices.
+  std::vector<int32_t> voff(nv + 1), vcid(topo_.nnz);
+  std::vector<double> vw(topo_.nnz);
+  std::vector<uint8_t> vbc(nv);
+  std::vector<Vec2<double>> vxy(nv);
+  voff[0] = 0;
+  for (int64_t v = 0; v < nv; ++v) {
+    const int64_t vo = vperm_[v];
+    const int64_t o0 = m.vert_coff[vo], o1 = m.vert_coff[vo + 1];
+    for (int64_t k = o0; k < o1; ++k) {
+      const int64_t j = voff[v] + (k - o0);
+      vcid[j] = (int32_t)cinv_[m.vert_wcells[k]];
+      vw[j] = m.vert_w[k];
+    }
+    voff[v + 1] = voff[v] + (int32_t)(o1 - o0);
+    vbc[v] = m.vbc[vo];
+    vxy[v] = Vec2<double>{m.vx[vo], m.vy[vo]};
+  }
+  // Wall edges in ascending reference id; cells owning them.
+  wall_edges_host_.clear();
+  std::vector<std::vector<int32_t>> wc_edges(nc);
+  std::vector<int32_t> wall_cells;
+  for (int64_t eo = 0; eo < ne; ++eo) {
+    if (m.ebc[eo] != 'w') continue;
+    wall_edges_host_.push_back((int32_t)einv_[eo]);
+    const int64_t c = cinv_[m.e_cl[eo]];
+    if (wc_edges[c].empty()) wall_cells.push_back((int32_t)c);
+    wc_edges[c].push_back((int32_t)einv_[eo]);
+  }
+  std::vector<int32_t> wc_off{0}, wc_list;
+  for (int32_t c : wall_cells) {
+    for (int32_t e : wc_edges[c]) wc_list.push_back(e);
+    wc_off.push_back((int32_t)wc_list.size());
+  }
+  // Shape-perturbation sets (src/shape_optimization.cpp:750-755,857-859).
+  std::vector<int32_t> pverts, pedges, pcells, pwverts;
+  std::vector<uint8_t> cmark(nc, 0), vmark(nv, 0);
+  for (int64_t v = 0; v < nv; ++v)
+    if (vbc[v] == 'w') pverts.push_back((int32_t)v);
+  for (int64_t e = 0; e < ne; ++e) {
+    if (ebc[e] == 'w' || vbc[ev[e].x] == 'w' || vbc[ev[e].y] == 'w') {
+      pedges.push_back((int32_t)e);
+      const int c = ec[e].x;
+      if (!cmark[c]) {
+        cmark[c] = 1;
+        pcells.push_back(c);
+      }
+    }
+  }
+  for (int32_t c : pcells)
+    for (int k = 0; k < ctype[c]; ++k) vmark[cverts[4 * c + k]] = 1;
+  for (int32_t v : pverts) vmark[v] = 1;
+  for (int64_t v = 0; v < nv; ++v)
+    if (vmark[v]) pwverts.push_back((int32_t)v);
+
+  // Device upload.
+  cudaStream_t s = stream_;
+  topo_.slot = arena_.alloc<int32_t>(slot.size());
+  topo_.jslot = arena_.alloc<int32_t>(jslot.size());
+  topo_.cverts = arena_.alloc<int32_t>(cverts.size());
+  topo_.ctype = arena_.alloc<uint8_t>(ctype.size());
+  topo_.ev = arena_.alloc<int2>(ne);
+  topo_.ec = arena_.alloc<int2>(ne);
+  topo_.ebc = arena_.alloc<uint8_t>(ne);
+  topo_.voff = arena_.alloc<int32_t>(nv + 1);
+  topo_.vcid = arena_.alloc<int32_t>(vcid.size());
+  topo_.vcid_ord = topo_.vcid;
+  topo_.vbc = arena_.alloc<uint8_t>(nv);
+  topo_.n_wall = (int64_t)wall_edges_host_.size();
+  topo_.wall_edges = arena_.alloc<int32_t>(wall_edges_host_.size());
+  topo_.n_wall_cells = (int64_t)wall_cells.size();
+  topo_.wall_cells = arena_.alloc<int32_t>(wall_cells.size());
+  topo_.wall_cell_off = arena_.alloc<int32_t>(wc_off.size());
+  topo_.wall_cell_edges = arena_.alloc<int32_t>(wc_list.size());
+  topo_.n_pert_verts = (int64_t)pverts.size();
+  topo_.pert_verts = arena_.alloc<int32_t>(pverts.size());
+  topo_.n_pert_edges = (int64_t)pedges.size();
+  topo_.pert_edges = arena_.alloc<int32_t>(pedges.size());
+  topo_.n_pert_cells = (int64_t)pcells.size();
+  topo_.pert_cells = arena_.alloc<int32_t>(pcells.size());
+  topo_.n_pert_wverts = (int64_t)pwverts.size();
+  topo_.pert_wverts = arena_.alloc<int32_t>(pwverts.size());
+  h2d(topo_.slot, slot, s);
+  h2d(topo_.jslot, jslot, s);
+  h2d(topo_.cverts, cverts, s);
+  h2d(topo_.ctype, ctype, s);
+  h2d(topo_.ev, ev, s);
+  h2d(topo_.ec, ec, s);
+  h2d(topo_.ebc, ebc, s);
+  h2d(topo_.voff, voff, s);
+  h2d(topo_.vcid, vcid, s);
+  h2d(topo_.vbc, vbc, s);
+  h2d(topo_.wall_edges, wall_edges_host_, s);
+  h2d(topo_.wall_cells, wall_cells, s);
+  h2d(topo_.wall_cell_off, wc_off, s);
+  h2d(topo_.wall_cell_edges, wc_list, s);
+  h2d(topo_.pert_verts, pverts, s);
+  h2d(topo_.pert_edges, pedges, s);
+  h2d(topo_.pert_cells, pcells, s);
+  h2d(topo_.pert_wverts, pwverts, s);
+
+  geom_.cgeom = arena_.alloc<Vec4<double>>(nc);
+  geom_.egeom = arena_.alloc<Vec4<double>>(ne);
+  geom_.ectr = arena_.alloc<Vec2<double>>(ne);
+  geom_.vxy = arena_.alloc<Vec2<double>>(nv);
+  geom_.vw = arena_.alloc<double>(vw.size());
+  h2d(geom_.cgeom, cgeom, s);
+  h2d(geom_.egeom, egeom, s);
+  h2d(geom_.ectr, ectr, s);
+  h2d(geom_.vxy, vxy, s);
+  h2d(geom_.vw, vw, s);
+
+  work_ = alloc_work();
+  U_ = arena_.alloc<Vec4<double>>(nc);
+  Uold_ = arena_.alloc<Vec4<double>>(nc);
+  norm_part_ = arena_.alloc<double>(grid(nc));
+  step_ = arena_.alloc<StepState>(1);
+  part_ = arena_.alloc<double>(kRedGrid * 4);
+  ticket_ = arena_.alloc<unsigned int>(4);
+  scal_ = arena_.alloc<double>(16);
+  ks_ = arena_.alloc<KrylovState>(1);
+  O2F_CUDA(cudaMemsetAsync(ticket_, 0, 4 * sizeof(unsigned int), s));
+  O2F_CUDA(cudaMemsetAsync(ks_, 0, sizeof(KrylovState), s));
+  sync();  // host staging vectors go out of scope
+}
+
+Work<double> Solver::alloc_work() {
+  Work<double> w{};
+  w.vq = arena_.alloc<Vec4<double>>(topo_.nv);
+  w.eL = arena_.alloc<Vec4<double>>(topo_.ne);
+  w.eR = arena_.alloc<Vec4<double>>(topo_.ne);
+  w.ctq = arena_.alloc<Vec4<double>>(topo_.nc);
+  w.ctqy = arena_.alloc<double>(topo_.nc);
+  w.vtq = arena_.alloc<Vec4<double>>(topo_.nv);
+  w.vtqy = arena_.alloc<double>(topo_.nv);
+  w.F = arena_.alloc<Vec4<double>>(topo_.ne);
+  w.etq = arena_.alloc<Vec4<double>>(topo_.ne);
+  w.etqy = arena_.alloc<double>(topo_.ne);
+  w.grad = arena_.alloc<Vec4<double>>(2 * topo_.nc);
+  w.R = arena_.alloc<Vec4<double>>(topo_.nc);
+  return w;
+}
+
+o2f_mesh_info Solver::info() const {
+  o2f_mesh_info i{};
+  i.n_cells = hm_.nc;
+  i.n_edges = hm_.ne;
+  i.n_vertices = hm_.nv;
+  i.n_wall_edges = topo_.n_wall;
+  int64_t nb = 0;
+  for (int64_t e = 0; e < hm_.ne; ++e) nb += hm_.e_cr[e] < 0;
+  i.n_boundary_edges = nb;
+  i.max_vertex_valence = hm_.max_valence;
+  i.min_h = min_h_;
+  i.device_bytes = arena_.bytes();
+  return i;
+}
+
+int64_t Solver::export_array(const std::string& w, void* out) const { return export_mesh_array(hm_, w, out); }
+
+void Solver::to_internal(const double* ref, Vec4<double>* dev) {
+  const int64_t nc = hm_.nc;
+  std::vector<Vec4<double>> tmp(nc);
+  for (int64_t c = 0; c < nc; ++c) {
+    const double* q = ref + 4 * cperm_[c];
+    tmp[c] = Vec4<double>{q[0], q[1], q[2], q[3]};
+  }
+  O2F_CUDA(cudaMemcpyAsync(dev, tmp.data(), nc * sizeof(Vec4<double>), cudaMemcpyHostToDevice, stream_));
+  sync();
+}
+
+void Solver::to_reference(const Vec4<double>* dev, double* ref) {
+  const int64_t nc = hm_.nc;
+  std::vector<Vec4<double>> tmp(nc);
+  O2F_CUDA(cudaMemcpyAsync(tmp.data(), dev, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  for (int64_t c = 0; c < nc; ++c) {
+    double* q = ref + 4 * cperm_[c];
+    q[0] = tmp[c].a;
+    q[1] = tmp[c].b;
+    q[2] = tmp[c].c;
+    q[3] = tmp[c].d;
+  }
+}
+
+void Solver::state_set(const double* U_ref) {
+  to_internal(U_ref, U_);
+  have_residual_ = false;
+  blk_valid_ = false;
+}
+
+void Solver::state_get(double* U_ref) { to_reference(U_, U_ref); }
+
+void Solver::state_freestream() {
+  // init_one_x (src/init.cpp:57-81) == the freestream boundary state.
+  std::vector<Vec4<double>> u(hm_.nc, Vec4<double>{phys_.fs_rho, phys_.fs_rhou, phys_.fs_rhov, phys_.fs_E});
+  O2F_CUDA(cudaMemcpyAsync(U_, u.data(), u.size() * sizeof(Vec4<double>), cudaMemcpyHostToDevice, stream_));
+  sync();
+  have_residual_ = false;
+  blk_valid_ = false;
+}
+
+void Solver::cell_permutation(int64_t* new_of_old) const {
+  std::memcpy(new_of_old, cinv_.data(), cinv_.size() * sizeof(int64_t));
+}
+
+void Solver::launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<double>* U, const int* gate,
+                             bool write_grad, const void* rkp) {
+  const Topo& t = topo_;
+  cudaStream_t s = stream_;
+  k_vertex_state<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, U, phys_, w.vq, gate);
+  if (write_grad)
+    k_cell_gradient<double, true><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
+                                                                w.eL, w.eR, w.ctq, w.ctqy, w.grad, gate);
+  else
+    k_cell_gradient<double, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
+                                                                 w.eL, w.eR, w.ctq, w.ctqy, w.grad, gate);
+  k_vertex_visc<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, w.ctq, w.ctqy, w.vtq,
+                                                      w.vtqy, gate);
+  k_edge_flux<double><<<grid(t.ne), kBlock, 0, s>>>(t.ne, g, t.ev, t.ebc, w.eL, w.eR, w.vtq, w.vtqy, phys_, w.F,
+                                                    w.etq, w.etqy, gate);
+  if (rkp) {
+    const RkStage rk = *static_cast<const RkStage*>(rkp);
+    k_cell_residual<double, true><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, w.F, w.etq, w.etqy, U, Uold_, w.R,
+                                                                rk, gate);
+  } else {
+    k_cell_residual<double, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, w.F, w.etq, w.etqy, U, Uold_,
+                                                                 w.R, RkStage{}, gate);
+  }
+  launches_ += 5;
+  O2F_CUDA(cudaGetLastError());
+}
+
+void Solver::residual(double* R_ref) {
+  O2F_CUDA(cudaEventRecord(ev0_, stream_));
+  launch_residual(geom_, work_, U_, nullptr, true, nullptr);
+  O2F_CUDA(cudaEventRecord(ev1_, stream_));
+  sync();
+  float ms = 0.f;
+  O2F_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  last_residual_ms_ = ms;
+  have_residual_ = true;
+  blk_valid_ = false;
+  if (R_ref) to_reference(work_.R, R_ref);
+}
+
+void Solver::debug_get(const std::string& which, double* out) {
+  if (!have_residual_) throw Error(O2F_ERR_STATE, "no residual has been evaluated");
+  const int64_t nc = hm_.nc, ne = hm_.ne, nv = hm_.nv;
+  if (which == "R") {
+    to_reference(work_.R, out);
+  } else if (which == "grad") {
+    std::vector<Vec4<double>> g(2 * nc);
+    O2F_CUDA(cudaMemcpy(g.data(), work_.grad, g.size() * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    for (int64_t c = 0; c < nc; ++c) {
+      double* q = out + 8 * cperm_[c];
+      const Vec4<double>&x = g[2 * c], &y = g[2 * c + 1];
+      const double vals[8] = {x.a, x.b, x.c, x.d, y.a, y.b, y.c, y.d};
+      std::memcpy(q, vals, sizeof(vals));
+    }
+  } else if (which == "edge_LR" || which == "edge_tau" || which == "edge_F") {
+    std::vector<Vec4<double>> L(ne), R(ne);
+    if (which == "edge_LR") {
+      O2F_CUDA(cudaMemcpy(L.data(), work_.eL, ne * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+      O2F_CUDA(cudaMemcpy(R.data(), work_.eR, ne * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    } else if (which == "edge_F") {
+      O2F_CUDA(cudaMemcpy(L.data(), work_.F, ne * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    } else {
+      O2F_CUDA(cudaMemcpy(L.data(), work_.etq, ne * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    }
+    for (int64_t e = 0; e < ne; ++e) {
+      const int64_t eo = eperm_[e];
+      if (which == "edge_LR") {
+        const double vals[8] = {L[e].a, L[e].b, L[e].c, L[e].d, R[e].a, R[e].b, R[e].c, R[e].d};
+        std::memcpy(out + 8 * eo, vals, sizeof(vals));
+      } else if (which == "edge_F") {
+        const double vals[4] = {L[e].a, L[e].b, L[e].c, L[e].d};
+        std::memcpy(out + 4 * eo, vals, sizeof(vals));
+      } else {
+        // The reference stores tau only on wall edges (src/diffusion.cpp:158-162).
+        const bool wall = hm_.ebc[eo] == 'w';
+        const double vals[3] = {wall ? L[e].a : 0.0, wall ? L[e].c : 0.0, wall ? L[e].b : 0.0};
+        std::memcpy(out + 3 * eo, vals, sizeof(vals));
+      }
+    }
+  } else if (which == "vertex_U") {
+    std::vector<Vec4<double>> q(nv);
+    O2F_CUDA(cudaMemcpy(q.data(), work_.vq, nv * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    for (int64_t v = 0; v < nv; ++v) {
+      double* o = out + 4 * vperm_[v];
+      o[0] = q[v].a;
+      o[1] = q[v].b;
+      o[2] = q[v].c;
+      o[3] = q[v].d;
+    }
+  } else {
+    throw Error(O2F_ERR_ARG, "unknown debug array '" + which + "'");
+  }
+}
+
+void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_t* steps_done, double* t_out) {
+  if (max_steps < 0) throw Error(O2F_ERR_ARG, "max_steps < 0");
+  if (hist_cap_ < std::max<int64_t>(max_steps, 1)) {
+    hist_cap_ = std::max<int64_t>(max_steps, 1);
+    hist_dev_ = arena_.alloc<double>(hist_cap_);
+  }
+  StepState st{};
+  st.t = 0.0;
+  st.final_time = params_.final_time;
+  st.cfl = params_.cfl_number;
+  st.min_h = min_h_;
+  st.mu = params_.viscosity;
+  st.drop_tol = drop_tol;
+  st.max_steps = max_steps;
+  O2F_CUDA(cudaMemcpyAsync(step_, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));
+  const int* gate = &step_->stop;
+  const double* dt = &step_->dt;
+  const RkStage s1{0.0, 1.0, dt, 1, norm_part_};
+  const RkStage s2{3.0 / 4.0, 1.0 / 4.0, dt, 0, nullptr};
+  const RkStage s3{1.0 / 3.0, 2.0 / 3.0, dt, 0, nullptr};
+  const int nparts = grid(topo_.nc);
+  const int wave_grid = std::min(grid(topo_.nc), 148 * 8);
+  // One CUDA graph holds kStepsPerGraph steps; steps past a stop condition
+  // are no-ops (every kernel checks the gate).
+  const int kStepsPerGraph = topo_.nc < 200000 ? 16 : 4;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  O2F_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < kStepsPerGraph; ++i) {
+    k_step_begin<<<1, 1, 0, stream_>>>(step_);
+    k_wave_speed<double><<<wave_grid, kBlock, 0, stream_>>>(topo_.nc, U_, params_.gamma, step_);
+    k_step_dt<<<1, 1, 0, stream_>>>(step_);
+    launch_residual(geom_, work_, U_, gate, false, &s1);
+    k_step_norm<<<1, 1024, 0, stream_>>>(norm_part_, nparts, hist_dev_, step_);
+    launch_residual(geom_, work_, U_, gate, false, &s2);
+    launch_residual(geom_, work_, U_, gate, false, &s3);
+    k_step_end<<<1, 1, 0, stream_>>>(step_);
+  }
+  O2F_CUDA(cudaStreamEndCapture(stream_, &graph));
+  O2F_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  StepState* host_st = nullptr;
+  O2F_CUDA(cudaMallocHost(&host_st, sizeof(StepState)));
+  int64_t launched = 0;
+  try {
+    while (true) {
+      O2F_CUDA(cudaGraphLaunch(exec, stream_));
+      launched += kStepsPerGraph;
+      launches_ += kStepsPerGraph * 20;
+      if (launched % (kStepsPerGraph * 4) == 0 || launched >= max_steps) {
+        O2F_CUDA(cudaMemcpyAsync(host_st, step_, sizeof(StepState), cudaMemcpyDeviceToHost, stream_));
+        sync();
+        if (host_st->stop) break;
+      }
+    }
+  } catch (...) {
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaFreeHost(host_st);
+    throw;
+  }
+  const StepState fin = *host_st;
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  cudaFreeHost(host_st);
+  if (history && fin.step > 0)
+    O2F_CUDA(cudaMemcpy(history, hist_dev_, std::min<int64_t>(fin.step, max_steps) * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  if (steps_done) *steps_done = fin.step;
+  if (t_out) *t_out = fin.t;
+  have_residual_ = fin.step > 0;
+  blk_valid_ = false;
+  if (fin.stop == 2) throw Error(O2F_ERR_NONFINITE, "non-finite state or residual in the time loop");
+}
+
+void Solver::forces(double beta, double* out3) {
+  if (!have_residual_) throw Error(O2F_ERR_STATE, "no residual has been evaluated");
+  k_forces<double><<<1, kBlock, 0, stream_>>>(topo_.n_wall, topo_.wall_edges, geom_, work_.eL, work_.etq, phys_,
+                                              beta, scal_);
+  O2F_CUDA(cudaGetLastError());
+  O2F_CUDA(cudaMemcpyAsync(out3, scal_, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  sync();
+}
+
+void Solver::build_jt_blocks() {
+  if (blk_valid_) return;
+  if (!have_residual_) throw Error(O2F_ERR_STATE, "no residual has been evaluated");
+  if (!blk_) blk_ = arena_.alloc<double>(32 * topo_.ne);
+  k_jt_blocks<<<(int)((topo_.ne + 127) / 128), 128, 0, stream_>>>(topo_.ne, geom_, topo_.ebc, work_.eL, work_.eR,
+                                                                   phys_, 1e-6, blk_);
+  O2F_CUDA(cudaGetLastError());
+  blk_valid_ = true;
+}
+
+void Solver::jt_apply_dev(const Vec4<double>* x, Vec4<double>* y) {
+  k_jt_apply<<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, x, y);
+  O2F_CUDA(cudaGetLastError());
+}
+
+void Solver::jt_apply(const double* x_ref, double* y_ref) {
+  build_jt_blocks();
+  if (!tmp_) tmp_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  if (!s_) s_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  to_internal(x_ref, s_);
+  jt_apply_dev(s_, tmp_);
+  to_reference(tmp_, y_ref);
+}
+
+void Solver::adjoint_rhs(double beta, double* b_ref) {
+  if (!have_residual_) throw Error(O2F_ERR_STATE, "no residual has been evaluated");
+  if (!b_) b_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  O2F_CUDA(cudaMemsetAsync(b_, 0, topo_.nc * sizeof(Vec4<double>), stream_));
+  if (topo_.n_wall_cells > 0)
+    k_adjoint_rhs<<<grid(topo_.n_wall_cells), kBlock, 0, stream_>>>(topo_.n_wall_cells, topo_.wall_cells,
+                                                                     topo_.wall_cell_off, topo_.wall_cell_edges,
+                                                                     geom_, work_.eL, phys_, beta, b_);
+  O2F_CUDA(cudaGetLastError());
+  if (b_ref) to_reference(b_, b_ref);
+}
+
+void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
+                           int64_t* iters, double* relres_out) {
+  if (!(tol > 0.0) || max_iter <= 0 || restart <= 0) throw Error(O2F_ERR_ARG, "invalid solver settings");
+  build_jt_blocks();
+  adjoint_rhs(beta, nullptr);
+  const int64_t nc = topo_.nc, n4 = 4 * nc;
+  auto need = [&](Vec4<double>*& p) {
+    if (!p) p = arena_.alloc<Vec4<double>>(nc);
+  };
+  need(lam_);
+  need(r_);
+  need(r0_);
+  need(p_);
+  need(v_);
+  need(s_);
+  need(t_);
+  need(tmp_);
+  double* x = reinterpret_cast<double*>(lam_);
+  O2F_CUDA(cudaMemsetAsync(lam_, 0, nc * sizeof(Vec4<double>), stream_));
+  // ||b||^2
+  k_dot2<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_), reinterpret_cast<double*>(b_), nullptr,
+                                           nullptr, part_, ticket_, scal_);
+  double bb[2];
+  O2F_CUDA(cudaMemcpyAsync(bb, scal_, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  const double bnorm = std::sqrt(bb[0]);
+  KrylovState ks{};
+  ks.tol2 = tol * tol * bb[0];
+  int64_t total = 0;
+  double relres = INFINITY;
+  const int kItersPerGraph = 8;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  O2F_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < kItersPerGraph; ++i) {
+    k_bicg_p<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_),
+                                               reinterpret_cast<double*>(p_), reinterpret_cast<double*>(v_), ks_);
+    k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, p_, v_, r0_,
+                                                  part_, ks_);
+    k_bicg_s<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(v_),
+                                               reinterpret_cast<double*>(s_), ks_);
+    k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, s_, t_, part_,
+                                                  ks_);
+    k_bicg_xr<<<kRedGrid, kBlock, 0, stream_>>>(n4, x, reinterpret_cast<double*>(p_), reinterpret_cast<double*>(s_),
+                                                reinterpret_cast<double*>(t_), reinterpret_cast<double*>(r_),
+                                                reinterpret_cast<double*>(r0_), part_, ks_);
+  }
+  O2F_CUDA(cudaStreamEndCapture(stream_, &graph));
+  O2F_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  KrylovState* hks = nullptr;
+  O2F_CUDA(cudaMallocHost(&hks, sizeof(KrylovState)));
+  int err = O2F_OK;
+  std::string msg;
+  try {
+    if (bb[0] == 0.0) {
+      relres = 0.0;
+    } else {
+      while (total < max_iter) {
+        // One restart chunk: solveWithGuess (src/shape_optimization.cpp:712).
+        ks.chunk_max = std::min<int64_t>(restart, max_iter - total);
+        ks.it = total;
+        O2F_CUDA(cudaMemcpyAsync(ks_, &ks, sizeof(KrylovState), cudaMemcpyHostToDevice, stream_));
+        jt_apply_dev(lam_, tmp_);
+        k_bicg_start<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_),
+                                                       reinterpret_cast<double*>(tmp_), reinterpret_cast<double*>(r_),
+                                                       reinterpret_cast<double*>(r0_), reinterpret_cast<double*>(p_),
+                                                       reinterpret_cast<double*>(v_), part_, ks_);
+        O2F_CUDA(cudaGetLastError());
+        int64_t launched = 0;
+        while (true) {
+          O2F_CUDA(cudaMemcpyAsync(hks, ks_, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream_));
+          sync();
+          if (hks->stop) break;
+          const int reps = launched < 64 ? 1 : 4;
+          for (int r = 0; r < reps; ++r) O2F_CUDA(cudaGraphLaunch(exec, stream_));
+          launched += reps * kItersPerGraph;
+          launches_ += reps * kItersPerGraph * 5;
+        }
+        const int64_t chunk_its = hks->it_chunk;
+        total += chunk_its;
+        // True residual (src/shape_optimization.cpp:716-717).
+        jt_apply_dev(lam_, tmp_);
+        k_bicg_start<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_),
+                                                       reinterpret_cast<double*>(tmp_), reinterpret_cast<double*>(s_),
+                                                       reinterpret_cast<double*>(t_), reinterpret_cast<double*>(p_),
+                                                       reinterpret_cast<double*>(v_), part_, ks_);
+        O2F_CUDA(cudaMemcpyAsync(hks, ks_, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream_));
+        sync();
+        relres = std::sqrt(hks->rr) / (bnorm > 0 ? bnorm : 1.0);
+        if (relres <= tol) break;
+        if (!std::isfinite(relres)) {
+          err = O2F_ERR_NONFINITE;
+          msg = "BiCGSTAB diverged";
+          break;
+        }
+        if (chunk_its == 0) {
+          err = O2F_ERR_BREAKDOWN;
+          msg = "BiCGSTAB breakdown";
+          break;
+        }
+      }
+      if (err == O2F_OK && relres > tol) {
+        err = O2F_ERR_NOT_CONVERGED;
+        msg = "BiCGSTAB did not converge";
+      }
+    }
+  } catch (...) {
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaFreeHost(hks);
+    throw;
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  cudaFreeHost(hks);
+  have_lambda_ = true;
+  if (iters) *iters = total;
+  if (relres_out) *relres_out = relres;
+  if (lambda_ref) to_reference(lam_, lambda_ref);
+  if (err != O2F_OK) throw Error(err, msg);
+}
+
+void Solver::ensure_pert_buffers() {
+  if (pert_alloc_) return;
+  pgeom_.cgeom = arena_.alloc<Vec4<double>>(topo_.nc);
+  pgeom_.egeom = arena_.alloc<Vec4<double>>(topo_.ne);
+  pgeom_.ectr = arena_.alloc<Vec2<double>>(topo_.ne);
+  pgeom_.vxy = arena_.alloc<Vec2<double>>(topo_.nv);
+  pgeom_.vw = arena_.alloc<double>(topo_.nnz);
+  pwork_ = alloc_work();
+  Rp_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  pert_alloc_ = true;
+}
+
+void Solver::perturbed_geometry(const o2f_shape_params& sp, int id, double eps) {
+  ensure_pert_buffers();
+  cudaStream_t s = stream_;
+  O2F_CUDA(cudaMemcpyAsync(pgeom_.cgeom, geom_.cgeom, topo_.nc * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, s));
+  O2F_CUDA(cudaMemcpyAsync(pgeom_.egeom, geom_.egeom, topo_.ne * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, s));
+  O2F_CUDA(cudaMemcpyAsync(pgeom_.ectr, geom_.ectr, topo_.ne * sizeof(Vec2<double>), cudaMemcpyDeviceToDevice, s));
+  O2F_CUDA(cudaMemcpyAsync(pgeom_.vxy, geom_.vxy, topo_.nv * sizeof(Vec2<double>), cudaMemcpyDeviceToDevice, s));
+  O2F_CUDA(cudaMemcpyAsync(pgeom_.vw, geom_.vw, topo_.nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ShapeArgs a{};
+  a.pos_x = sp.pos_x;
+  a.c = sp.c;
+  a.m0 = sp.m;
+  a.p0 = sp.p;
+  a.t0 = sp.t;
+  a.m1 = sp.m;
+  a.p1 = sp.p;
+  a.t1 = sp.t;
+  if (id == O2F_PARAM_M)
+    a.m1 = sp.m + eps;
+  else if (id == O2F_PARAM_P)
+    a.p1 = sp.p + eps;
+  else if (id == O2F_PARAM_T)
+    a.t1 = sp.t + eps;
+  else
+    throw Error(O2F_ERR_ARG, "unknown shape parameter id");
+  const Topo& t = topo_;
+  if (t.n_pert_verts)
+    k_perturb_vertices<<<grid(t.n_pert_verts), kBlock, 0, s>>>(t.n_pert_verts, t.pert_verts, a, pgeom_.vxy);
+  if (t.n_pert_cells)
+    k_perturb_cells<double><<<grid(t.n_pert_cells), kBlock, 0, s>>>(t.n_pert_cells, t.pert_cells, t.cverts, t.ctype,
+                                                                     t.nc, pgeom_.vxy, params_.limiter_k, pgeom_.cgeom);
+  if (t.n_pert_edges)
+    k_perturb_edges<double><<<grid(t.n_pert_edges), kBlock, 0, s>>>(t.n_pert_edges, t.pert_edges, t.ev, t.ec,
+                                                                     pgeom_.vxy, pgeom_.cgeom, pgeom_.egeom,
+                                                                     pgeom_.ectr);
+  if (t.n_pert_wverts)
+    k_vertex_weights<double><<<grid(t.n_pert_wverts), kBlock, 0, s>>>(t.n_pert_wverts, t.pert_wverts, t.voff, t.vcid,
+                                                                       t.vcid, t.vbc, pgeom_.vxy, pgeom_.cgeom,
+                                                                       pgeom_.vw);
+  O2F_CUDA(cudaGetLastError());
+}
+
+void Solver::shape_gradient(const o2f_shape_params& sp, const int* ids, int n, double beta, double eps,
+                            const double* lambda_ref, double* grad) {
+  if (n < 0 || (n > 0 && (!ids || !grad))) throw Error(O2F_ERR_ARG, "invalid parameter list");
+  if (!(eps > 0.0)) throw Error(O2F_ERR_ARG, "eps must be positive");
+  if (!lam_) lam_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  if (lambda_ref) {
+    to_internal(lambda_ref, lam_);
+  } else if (!have_lambda_) {
+    throw Error(O2F_ERR_STATE, "no adjoint solution: solve first or pass lambda");
+  }
+  // computeShapeGradient starts with a residual of the unperturbed mesh (:955-956).
+  launch_residual(geom_, work_, U_, nullptr, false, nullptr);
+  have_residual_ = true;
+  blk_valid_ = false;
+  for (int k = 0; k < n; ++k) {
+    double J[2];
+    for (int sgn = 0; sgn < 2; ++sgn) {
+      perturbed_geometry(sp, ids[k], sgn == 0 ? eps : -eps);
+      launch_residual(pgeom_, pwork_, U_, nullptr, false, nullptr);
+      k_forces<double><<<1, kBlock, 0, stream_>>>(topo_.n_wall, topo_.wall_edges, pgeom_, pwork_.eL, pwork_.etq,
+                                                  phys_, beta, scal_ + 4 + 4 * sgn);
+      if (sgn == 0)
+        O2F_CUDA(cudaMemcpyAsync(Rp_, pwork_.R, topo_.nc * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, stream_));
+    }
+    k_lambda_dR<double><<<kRedGrid, kBlock, 0, stream_>>>(topo_.nc, lam_, Rp_, pwork_.R, 2.0 * eps, part_, ticket_,
+                                                          scal_ + 12);
+    O2F_CUDA(cudaGetLastError());
+    double h[16];
+    O2F_CUDA(cudaMemcpyAsync(h, scal_, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    sync();
+    J[0] = h[4 + 2];
+    J[1] = h[8 + 2];
+    const double dJ_direct = (J[0] - J[1]) / (2.0 * eps);
+    grad[k] = dJ_direct - h[12];
+  }
+}
+
+void Solver::debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which,
+                             double* out) {
+  perturbed_geometry(sp, id, eps);
+  sync();
+  const int64_t nc = hm_.nc, ne = hm_.ne, nv = hm_.nv;
+  if (which == "cell_vol" || which == "cell_ctr") {
+    std::vector<Vec4<double>> g(nc);
+    O2F_CUDA(cudaMemcpy(g.data(), pgeom_.cgeom, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    for (int64_t c = 0; c < nc; ++c) {
+      const int64_t co = cperm_[c];
+      if (which == "cell_vol") {
+        out[co] = g[c].c;
+      } else {
+        out[2 * co] = g[c].a;
+        out[2 * co + 1] = g[c].b;
+      }
+    }
+  } else if (which == "edge_len" || which == "edge_n" || which == "edge_ctr") {
+    std::vector<Vec4<double>> g(ne);
+    std::vector<Vec2<double>> ce(ne);
+    O2F_CUDA(cudaMemcpy(g.data(), pgeom_.egeom, ne * sizeof(Vec4<double>), cudaMemcpyDeviceToHost));
+    O2F_CUDA(cudaMemcpy(ce.data(), pgeom_.ectr, ne * sizeof(Vec2<double>), cudaMemcpyDeviceToHost));
+    for (int64_t e = 0; e < ne; ++e) {
+      const int64_t eo = eperm_[e];
+      if (which == "edge_len") {
+        out[eo] = g[e].c;
+      } else if (which == "edge_n") {
+        out[2 * eo] = g[e].a;
+        out[2 * eo + 1] = g[e].b;
+      } else {
+        out[2 * eo] = ce[e].a;
+        out[2 * eo + 1] = ce[e].b;
+      }
+    }
+  } else if (which == "vert_xy") {
+    std::vector<Vec2<double>> g(nv);
+    O2F_CUDA(cudaMemcpy(g.data(), pgeom_.vxy, nv * sizeof(Vec2<double>), cudaMemcpyDeviceToHost));
+    for (int64_t v = 0; v < nv; ++v) {
+      out[2 * vperm_[v]] = g[v].a;
+      out[2 * vperm_[v] + 1] = g[v].b;
+    }
+  } else if (which == "vert_w") {
+    std::vector<double> w(topo_.nnz);
+    O2F_CUDA(cudaMemcpy(w.data(), pgeom_.vw, w.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int32_t> voff(nv + 1);
+    // Rebuild the internal CSR offsets to map back to reference order.
+    int64_t acc = 0;
+    for (int64_t v = 0; v < nv; ++v) {
+      voff[v] = (int32_t)acc;
+      acc += hm_.vert_coff[vperm_[v] + 1] - hm_.vert_coff[vperm_[v]];
+    }
+    for (int64_t v = 0; v < nv; ++v) {
+      const int64_t vo = vperm_[v];
+      for (int64_t k = hm_.vert_coff[vo]; k < hm_.vert_coff[vo + 1]; ++k)
+        out[k] = w[voff[v] + (k - hm_.vert_coff[vo])];
+    }
+  } else {
+    throw Error(O2F_ERR_ARG, "unknown perturbed array '" + which + "'");
+  }
+}
+
+}  // namespace o2f

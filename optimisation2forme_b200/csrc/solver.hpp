@@ -1,0 +1,128 @@
+// The solver context behind the C ABI: device-resident renumbered mesh, state,
+// interface states of the last residual, adjoint vectors and all scratch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "device_types.hpp"
+#include "mesh_host.hpp"
+#include "o2f.h"
+
+namespace o2f {
+
+struct KrylovState;
+struct StepState;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define O2F_CUDA(x) ::o2f::cuda_check((x), #x)
+
+// Owning device allocation list.
+class DeviceArena {
+ public:
+  ~DeviceArena();
+  template <typename X>
+  X* alloc(size_t n) {
+    return static_cast<X*>(raw(n * sizeof(X)));
+  }
+  void* raw(size_t bytes);
+  size_t bytes() const { return bytes_; }
+
+ private:
+  std::vector<void*> ptrs_;
+  size_t bytes_ = 0;
+};
+
+class Solver {
+ public:
+  Solver(const o2f_mesh_desc& desc, const o2f_params& p, cudaStream_t stream);
+  ~Solver();
+
+  void set_params(const o2f_params& p);
+  o2f_mesh_info info() const;
+  int64_t export_array(const std::string& which, void* out) const;
+
+  void state_set(const double* U_ref);
+  void state_get(double* U_ref);
+  void state_freestream();
+  double* state_device() { return reinterpret_cast<double*>(U_); }
+  void cell_permutation(int64_t* new_of_old) const;
+
+  void residual(double* R_ref);
+  void debug_get(const std::string& which, double* out);
+  void rk3_run(int64_t max_steps, double drop_tol, double* history, int64_t* steps_done, double* t_out);
+  void forces(double beta, double* out3);
+  void jt_apply(const double* x_ref, double* y_ref);
+  void adjoint_rhs(double beta, double* b_ref);
+  void adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
+                     int64_t* iters, double* relres);
+  void shape_gradient(const o2f_shape_params& sp, const int* ids, int n, double beta, double eps,
+                      const double* lambda_ref, double* grad);
+  void debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which, double* out);
+  double last_residual_ms() const { return last_residual_ms_; }
+  int64_t launches() const { return launches_; }
+
+ private:
+  void upload_mesh();
+  void compute_phys();
+  void launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<double>* U, const int* gate,
+                       bool write_grad, const void* rk);
+  void build_jt_blocks();
+  void jt_apply_dev(const Vec4<double>* x, Vec4<double>* y);
+  void perturbed_geometry(const o2f_shape_params& sp, int id, double eps);
+  void ensure_pert_buffers();
+  Work<double> alloc_work();
+  void to_internal(const double* ref, Vec4<double>* dev);
+  void to_reference(const Vec4<double>* dev, double* ref);
+  void sync();
+  int grid(int64_t n) const { return (int)((n + 255) / 256); }
+
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  o2f_params params_{};
+  Phys phys_{};
+  HostMesh hm_;
+  double min_h_ = 0.0;
+  std::vector<int64_t> cperm_, cinv_, eperm_, einv_, vperm_, vinv_;
+  std::vector<int32_t> wall_edges_host_;
+  DeviceArena arena_;
+  Topo topo_{};
+  Geom<double> geom_{};
+  Work<double> work_{};
+  Vec4<double>* U_ = nullptr;
+  Vec4<double>* Uold_ = nullptr;
+  double* norm_part_ = nullptr;
+  StepState* step_ = nullptr;
+  double* hist_dev_ = nullptr;
+  int64_t hist_cap_ = 0;
+  // adjoint
+  double* blk_ = nullptr;
+  bool blk_valid_ = false;
+  bool have_residual_ = false;
+  bool have_lambda_ = false;
+  Vec4<double>*lam_ = nullptr, *b_ = nullptr, *r_ = nullptr, *r0_ = nullptr, *p_ = nullptr, *v_ = nullptr,
+  *s_ = nullptr, *t_ = nullptr, *tmp_ = nullptr;
+  KrylovState* ks_ = nullptr;
+  double* part_ = nullptr;
+  unsigned int* ticket_ = nullptr;
+  double* scal_ = nullptr;  // small device scalars
+  // shape perturbation
+  Geom<double> pgeom_{};
+  Work<double> pwork_{};
+  Vec4<double>* Rp_ = nullptr;
+  bool pert_alloc_ = false;
+  double last_residual_ms_ = 0.0;
+  int64_t launches_ = 0;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+};
+
+}  // namespace o2f

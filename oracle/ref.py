@@ -1,0 +1,66 @@
+"""Test infrastructure only: runs the reference solver's own code (built by
+oracle/build_ref.sh into oracle/_ref/) as a subprocess and reads its dumps.
+
+One process per call, because the reference sizes function-static scratch
+buffers on its first residual (src/advection.cpp:9-23, src/diffusion.cpp:9-25).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = Path(os.environ.get("O2F_REFERENCE_DIR", "/root/reference"))
+EXE_EXACT = HERE / "_ref" / "o2f_ref_exact"
+EXE_FAST = HERE / "_ref" / "o2f_ref_fast"
+
+
+def available() -> bool:
+    return EXE_EXACT.exists()
+
+
+def build() -> bool:
+    """Compile the reference from its sources when they are present."""
+    if (REF_DIR / "src" / "advection.cpp").exists():
+        subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True, env={**os.environ, "REF_DIR": str(REF_DIR)},
+                       capture_output=True)
+        return True
+    return False
+
+
+def write_config(path: Path, *, mesh: str, state: str = "", params_file: str = "", viscosity=1.8e-5,
+                 inflow_velocity=0.3, cfl=0.5, final_time=0.005, Pr=0.71, extra: str = "") -> Path:
+    """A reference config file (keys of src/params.cpp:35-77)."""
+    txt = (f"viscosity = {viscosity!r}\nPr = {Pr!r}\ncfl_number = {cfl!r}\nfinal_time = {final_time!r}\n"
+           f"verbosity = 0\nreload_config = 0\ninitial_condition = one_x\nboundary_conditions = inflow_outflow_x\n"
+           f"noise_level = 0\ninflow_velocity = {inflow_velocity!r}\nmesh_name = {mesh}\n")
+    if state:
+        txt += f"state_load_path = {state}\n"
+    if params_file:
+        txt += f"shape_param_file = {params_file}\n"
+    Path(path).write_text(txt + extra)
+    return Path(path)
+
+
+def run(mode: str, config: Path, *args: str, exact: bool = True, threads: int = 1, capture=False) -> dict:
+    """Run one harness mode; returns {name: array} of its dumps (or stdout)."""
+    exe = EXE_EXACT if exact else EXE_FAST
+    with tempfile.TemporaryDirectory() as td:
+        env = {**os.environ, "OMP_NUM_THREADS": str(threads)}
+        r = subprocess.run([str(exe), mode, str(config), td, *map(str, args)], cwd=td, env=env, capture_output=True,
+                           text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({mode}): {r.stderr.strip()}")
+        if capture:
+            return {"stdout": r.stdout}
+        out = {}
+        for f in Path(td).iterdir():
+            if f.suffix == ".f64":
+                out[f.stem] = np.fromfile(f, dtype=np.float64)
+            elif f.suffix == ".i64":
+                out[f.stem] = np.fromfile(f, dtype=np.int64)
+        return out

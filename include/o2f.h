@@ -63,6 +63,13 @@ typedef enum o2f_status {
 #define O2F_LIMITER_VENKAT 0
 #define O2F_LIMITER_BARTH_JESPERSEN 1
 
+/* Preconditioner of the adjoint BiCGSTAB.  NONE is the reference's
+ * Eigen::IdentityPreconditioner (src/shape_optimization.cpp:699); ILU0 is a
+ * block (4x4) ILU(0) of J^T in reverse Cuthill-McKee order.  Both solve the
+ * same system to the same true-residual tolerance. */
+#define O2F_PRECOND_NONE 0
+#define O2F_PRECOND_ILU0 1
+
 /* Arithmetic of the residual / Jacobian-transpose kernels. */
 #define O2F_PREC_F64 0 /* FP64 throughout (parity mode)                           */
 #define O2F_PREC_F32 1 /* FP32 residual and JT, FP64 reductions, dt and Krylov     */
@@ -86,6 +93,9 @@ typedef struct o2f_params {
   double limiter_k;       /* NEW: Venkatakrishnan K, eps=(K h)^3; reference 1e-2 */
   int limiter;            /* NEW: O2F_LIMITER_*                                */
   int precision;          /* NEW: O2F_PREC_*                                   */
+  int adjoint_precond;    /* NEW: O2F_PRECOND_* (default ILU0)                 */
+  int verbosity;          /* >= 1: "[adjoint] iters=.. relres=.." per restart chunk
+                             on stderr, as src/shape_optimization.cpp:719 prints */
 } o2f_params;
 
 void o2f_params_default(o2f_params* p);
@@ -236,12 +246,29 @@ int o2f_debug_perturbed(o2f_ctx* ctx, const o2f_shape_params* shape, int param_i
 int o2f_state_device(o2f_ctx* ctx, double** U_dev);
 int o2f_cell_permutation(const o2f_ctx* ctx, int64_t* new_of_old_host);
 
-/* Timing of the last o2f_rk3_run / o2f_adjoint_solve, per kernel class. */
+/* Timing of the last o2f_residual and the number of kernels launched so far. */
 typedef struct o2f_timing {
   double residual_ms;  /* last o2f_residual */
   int64_t kernel_launches;
 } o2f_timing;
 int o2f_get_timing(const o2f_ctx* ctx, o2f_timing* t);
+
+/* Kernel classes timed by o2f_profile_kernels (no reference counterpart:
+ * per-kernel CUDA-event timing replaces the reference's wall-clock
+ * time_tic/time_toc printouts, src/utils.cpp:13-23). */
+#define O2F_K_VERTEX_STATE 0  /* cell -> vertex state interpolation          */
+#define O2F_K_CELL_GRADIENT 1 /* Green-Gauss, limiter, interface states, tau  */
+#define O2F_K_VERTEX_VISC 2   /* cell -> vertex tau/q interpolation           */
+#define O2F_K_EDGE_FLUX 3     /* HLLC + edge viscous values                   */
+#define O2F_K_CELL_RESIDUAL 4 /* residual gather + viscous divergence         */
+#define O2F_K_JT_APPLY 5      /* matrix-free J^T x                            */
+#define O2F_K_JT_BLOCKS 6     /* finite-difference flux Jacobian blocks       */
+#define O2F_K_COUNT 7
+/* Launches each kernel class `reps` times back to back on the context stream
+ * (about the current state) and writes the mean duration of one launch in
+ * milliseconds, measured with CUDA events on that stream, to
+ * ms_out[O2F_K_COUNT]. */
+int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out);
 
 #ifdef __cplusplus
 }

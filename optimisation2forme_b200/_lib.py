@@ -53,6 +53,8 @@ class Params(C.Structure):
         ("limiter_k", C.c_double),
         ("limiter", C.c_int),
         ("precision", C.c_int),
+        ("adjoint_precond", C.c_int),
+        ("verbosity", C.c_int),
     ]
 
 
@@ -128,7 +130,11 @@ SIGNATURES = {
     "o2f_state_device": ([_vp, C.POINTER(_dp)], C.c_int),
     "o2f_cell_permutation": ([_vp, _ip], C.c_int),
     "o2f_get_timing": ([_vp, C.POINTER(Timing)], C.c_int),
+    "o2f_profile_kernels": ([_vp, C.c_int, _dp], C.c_int),
 }
+
+KERNEL_CLASSES = ["vertex_state", "cell_gradient", "vertex_visc", "edge_flux", "cell_residual", "jt_apply",
+                  "jt_blocks"]
 
 _lib = None
 

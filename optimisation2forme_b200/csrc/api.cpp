@@ -90,6 +90,8 @@ void o2f_params_default(o2f_params* p) {
   p->limiter_k = 1e-2;  // k_eps of computeVenkatAlpha (src/advection.cpp:209)
   p->limiter = O2F_LIMITER_VENKAT;
   p->precision = O2F_PREC_F64;
+  p->adjoint_precond = O2F_PRECOND_ILU0;
+  p->verbosity = 0;
 }
 
 int o2f_host_mesh_create(const o2f_mesh_desc* mesh, o2f_host_mesh** out) {
@@ -304,6 +306,13 @@ int o2f_cell_permutation(const o2f_ctx* ctx, int64_t* new_of_old_host) {
   return guarded([&] {
     need(new_of_old_host, "out");
     S(ctx).cell_permutation(new_of_old_host);
+  });
+}
+
+int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out) {
+  return guarded([&] {
+    need(ms_out, "ms_out");
+    S(ctx).profile_kernels(reps, ms_out);
   });
 }
 

@@ -100,6 +100,20 @@ struct Phys {
   int limiter;
 };
 
+// Block ILU(0) preconditioner of the adjoint operator (see ilu.cuh).
+struct IluDev {
+  int64_t nc;
+  int32_t* nbr;     // [4*nc] neighbour cell of each slot (slot order = jslot order), -1 if none
+  int32_t* pos;     // [nc] position of the cell in the ILU order
+  double* A;        // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
+  double* Dinv;     // [nc*16]
+  int32_t* lo_off;  // [n_lo+1] forward levels
+  int32_t* lo_cells;
+  int32_t* up_off;  // [n_up+1] backward levels
+  int32_t* up_cells;
+  int n_lo, n_up;
+};
+
 // Buffers written by one residual evaluation.
 template <typename T>
 struct Work {

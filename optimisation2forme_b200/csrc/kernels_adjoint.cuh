@@ -472,17 +472,19 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(int64_t n4, const double* __r
     s[i] = r[i] - alpha * v[i];
 }
 
-// t = J^T s with the fused dots (t, t), (t, s); epilogue omega.
+// t = J^T shat (shat = M^{-1} s, or s itself without preconditioner) with the
+// fused dots (t, t), (t, s); epilogue omega.
 __global__ void __launch_bounds__(kBlock) k_bicg_jt_t(int64_t nc, const int32_t* __restrict__ jslot, Geom<double> g,
                                                       const int2* __restrict__ ec, const uint8_t* __restrict__ ebc,
                                                       const double* __restrict__ blk,
+                                                      const Vec4<double>* __restrict__ shat,
                                                       const Vec4<double>* __restrict__ s, Vec4<double>* __restrict__ t,
                                                       double* part, KrylovState* ks) {
   if (ks->stop) return;
   double acc[2] = {0.0, 0.0};
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
     Vec4<double> y;
-    jt_cell<0>(c, nc, jslot, g, ec, ebc, blk, s, y);
+    jt_cell<0>(c, nc, jslot, g, ec, ebc, blk, shat, y);
     t[c] = y;
     const Vec4<double> q = s[c];
     acc[0] += y.a * y.a + y.b * y.b + y.c * y.c + y.d * y.d;
@@ -492,9 +494,10 @@ __global__ void __launch_bounds__(kBlock) k_bicg_jt_t(int64_t nc, const int32_t*
   if (grid_reduce<2>(acc, part, &ks->ticket, tot)) ks->omega = (tot[0] > 0.0) ? tot[1] / tot[0] : 0.0;
 }
 
-// x += alpha p + omega s; r = s - omega t; dots (r0, r), (r, r); epilogue:
-// convergence test, restart test, next beta.
-__global__ void __launch_bounds__(kBlock) k_bicg_xr(int64_t n4, double* __restrict__ x, const double* __restrict__ p,
+// x += alpha phat + omega shat; r = s - omega t; dots (r0, r), (r, r);
+// epilogue: convergence test, restart test, next beta.
+__global__ void __launch_bounds__(kBlock) k_bicg_xr(int64_t n4, double* __restrict__ x,
+                                                    const double* __restrict__ phat, const double* __restrict__ shat,
                                                     const double* __restrict__ s, const double* __restrict__ t,
                                                     double* __restrict__ r, const double* __restrict__ r0,
                                                     double* part, KrylovState* ks) {
@@ -503,7 +506,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_xr(int64_t n4, double* __restri
   double acc[2] = {0.0, 0.0};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
     const double si = s[i];
-    x[i] = x[i] + alpha * p[i] + omega * si;
+    x[i] = x[i] + alpha * phat[i] + omega * shat[i];
     const double ri = si - omega * t[i];
     r[i] = ri;
     acc[0] += r0[i] * ri;
@@ -721,6 +724,13 @@ __global__ void k_vertex_weights(int64_t n, const int32_t* __restrict__ verts, c
     for (int k = 0; k < nn; ++k) wsum += w[k];
     for (int k = 0; k < nn; ++k) vw[o + k] = (T)(w[k] / wsum);
   }
+}
+
+// Uniform state fill (init_one_x, src/init.cpp:57-81), on the device.
+template <typename T>
+__global__ void k_fill_state(int64_t nc, Vec4<T> v, Vec4<T>* __restrict__ U) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nc) U[c] = v;
 }
 
 // Venkatakrishnan eps = (k h)^3, h = sqrt(V / pi) (src/advection.cpp:214-215).

@@ -4,9 +4,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 
+#include "ilu.cuh"
 #include "kernels_adjoint.cuh"
 
 namespace o2f {
@@ -42,6 +44,8 @@ void validate_params(const o2f_params& p) {
   if (p.limiter != O2F_LIMITER_VENKAT && p.limiter != O2F_LIMITER_BARTH_JESPERSEN)
     throw Error(O2F_ERR_ARG, "unknown limiter");
   if (p.precision != O2F_PREC_F64) throw Error(O2F_ERR_ARG, "this context supports O2F_PREC_F64");
+  if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
+    throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
 }
 
 }  // namespace
@@ -315,6 +319,167 @@ void Solver::upload_mesh() {
   O2F_CUDA(cudaMemsetAsync(ticket_, 0, 4 * sizeof(unsigned int), s));
   O2F_CUDA(cudaMemsetAsync(ks_, 0, sizeof(KrylovState), s));
   sync();  // host staging vectors go out of scope
+  setup_ilu_host(jslot, ec, ebc);
+}
+
+// Reverse Cuthill-McKee order of the cell adjacency graph (BFS from a
+// pseudo-peripheral cell, neighbours by increasing degree, reversed), and the
+// level sets of the forward / backward triangular solves in that order.
+void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector<int2>& ec,
+                            const std::vector<uint8_t>& ebc) {
+  const int64_t nc = topo_.nc;
+  ilu_nbr_h_.assign(4 * nc, -1);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int k = 0; k < 4; ++k) {
+      const int sl = jslot[k * nc + c];
+      if (sl < 0) continue;
+      const int e = sl >> 1;
+      if (ebc[e] != 0) continue;
+      ilu_nbr_h_[k * nc + c] = (sl & 1) == 0 ? ec[e].y : ec[e].x;
+    }
+  auto nbr = [&](int64_t c, int k) { return ilu_nbr_h_[k * nc + c]; };
+  std::vector<int> deg(nc, 0);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int k = 0; k < 4; ++k) deg[c] += nbr(c, k) >= 0;
+  std::vector<int> seen(nc, 0);
+  std::vector<int32_t> lvl(nc);
+  int stamp = 0;
+  auto bfs = [&](int32_t root, std::vector<int32_t>& out) {  // BFS order into out, depth into lvl
+    out.clear();
+    out.push_back(root);
+    lvl[root] = 0;
+    ++stamp;
+    seen[root] = stamp;
+    for (size_t h = 0; h < out.size(); ++h) {
+      const int32_t u = out[h];
+      int32_t nb[4];
+      int n = 0;
+      for (int k = 0; k < 4; ++k) {
+        const int32_t v = nbr(u, k);
+        if (v >= 0 && seen[v] != stamp) nb[n++] = v;
+      }
+      std::sort(nb, nb + n, [&](int32_t a, int32_t b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+      for (int i = 0; i < n; ++i) {
+        if (seen[nb[i]] == stamp) continue;
+        seen[nb[i]] = stamp;
+        lvl[nb[i]] = lvl[u] + 1;
+        out.push_back(nb[i]);
+      }
+    }
+  };
+  std::vector<int32_t> order;
+  order.reserve(nc);
+  std::vector<char> placed(nc, 0);
+  std::vector<int32_t> comp;
+  for (int64_t start = 0; start < nc; ++start) {
+    if (placed[start]) continue;
+    // pseudo-peripheral root: repeat the BFS from the farthest low-degree cell
+    int32_t root = (int32_t)start;
+    int depth = -1;
+    for (int it = 0; it < 4; ++it) {
+      bfs(root, comp);
+      const int d = lvl[comp.back()];
+      if (d <= depth) break;
+      depth = d;
+      int32_t best = comp.back();
+      for (auto r = comp.rbegin(); r != comp.rend() && lvl[*r] == d; ++r)
+        if (deg[*r] < deg[best]) best = *r;
+      root = best;
+    }
+    bfs(root, comp);
+    for (int32_t c : comp) placed[c] = 1;
+    order.insert(order.end(), comp.begin(), comp.end());
+  }
+  std::reverse(order.begin(), order.end());
+  ilu_pos_h_.assign(nc, 0);
+  for (int64_t i = 0; i < nc; ++i) ilu_pos_h_[order[i]] = (int32_t)i;
+  std::vector<int32_t> lev(nc, 0);
+  auto bucket = [&](int nl, std::vector<int32_t>& off, std::vector<int32_t>& cells) {
+    off.assign(nl + 1, 0);
+    for (int64_t c = 0; c < nc; ++c) off[lev[c] + 1]++;
+    for (int l = 0; l < nl; ++l) off[l + 1] += off[l];
+    cells.assign(nc, 0);
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (int64_t i = 0; i < nc; ++i) cells[fill[lev[order[i]]]++] = order[i];
+  };
+  int nlo = 0;
+  for (int64_t i = 0; i < nc; ++i) {
+    const int32_t c = order[i];
+    int l = 0;
+    for (int k = 0; k < 4; ++k) {
+      const int32_t o = nbr(c, k);
+      if (o >= 0 && ilu_pos_h_[o] < i) l = std::max(l, lev[o] + 1);
+    }
+    lev[c] = l;
+    nlo = std::max(nlo, l + 1);
+  }
+  bucket(nlo, lo_off_h_, lo_cells_h_);
+  int nup = 0;
+  for (int64_t i = nc - 1; i >= 0; --i) {
+    const int32_t c = order[i];
+    int l = 0;
+    for (int k = 0; k < 4; ++k) {
+      const int32_t o = nbr(c, k);
+      if (o >= 0 && ilu_pos_h_[o] > i) l = std::max(l, lev[o] + 1);
+    }
+    lev[c] = l;
+    nup = std::max(nup, l + 1);
+  }
+  bucket(nup, up_off_h_, up_cells_h_);
+  ilu_.nc = nc;
+  ilu_.n_lo = nlo;
+  ilu_.n_up = nup;
+}
+
+void Solver::ilu_factor() {
+  const int64_t nc = topo_.nc;
+  cudaStream_t s = stream_;
+  if (!ilu_alloc_) {
+    ilu_.nbr = arena_.alloc<int32_t>(4 * nc);
+    ilu_.pos = arena_.alloc<int32_t>(nc);
+    ilu_.A = arena_.alloc<double>(80 * nc);
+    ilu_.Dinv = arena_.alloc<double>(16 * nc);
+    ilu_.lo_off = arena_.alloc<int32_t>(lo_off_h_.size());
+    ilu_.lo_cells = arena_.alloc<int32_t>(nc);
+    ilu_.up_off = arena_.alloc<int32_t>(up_off_h_.size());
+    ilu_.up_cells = arena_.alloc<int32_t>(nc);
+    ilu_status_ = arena_.alloc<int>(1);
+    phat_ = arena_.alloc<Vec4<double>>(nc);
+    shat_ = arena_.alloc<Vec4<double>>(nc);
+    h2d(ilu_.nbr, ilu_nbr_h_, s);
+    h2d(ilu_.pos, ilu_pos_h_, s);
+    h2d(ilu_.lo_off, lo_off_h_, s);
+    h2d(ilu_.lo_cells, lo_cells_h_, s);
+    h2d(ilu_.up_off, up_off_h_, s);
+    h2d(ilu_.up_cells, up_cells_h_, s);
+    sync();
+    ilu_alloc_ = true;
+  }
+  O2F_CUDA(cudaMemsetAsync(ilu_status_, 0, sizeof(int), s));
+  k_ilu_assemble<<<grid(nc), kBlock, 0, s>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ilu_);
+  for (int l = 0; l < ilu_.n_lo; ++l) {
+    const int n = lo_off_h_[l + 1] - lo_off_h_[l];
+    k_ilu_factor<<<(n + 127) / 128, 128, 0, s>>>(ilu_.lo_cells + lo_off_h_[l], n, ilu_, ilu_status_);
+  }
+  O2F_CUDA(cudaGetLastError());
+  launches_ += 1 + ilu_.n_lo;
+  int st = 0;
+  O2F_CUDA(cudaMemcpyAsync(&st, ilu_status_, sizeof(int), cudaMemcpyDeviceToHost, s));
+  sync();
+  if (st) throw Error(O2F_ERR_BREAKDOWN, "singular block in the ILU(0) factorization");
+}
+
+// z = M^{-1} r: forward levels into z, backward levels in place.
+void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) {
+  cudaStream_t s = stream_;
+  for (int l = 0; l < ilu_.n_lo; ++l) {
+    const int n = lo_off_h_[l + 1] - lo_off_h_[l];
+    k_ilu_lower<<<(n + 127) / 128, 128, 0, s>>>(ilu_.lo_cells + lo_off_h_[l], n, ilu_, r, z, gate);
+  }
+  for (int l = 0; l < ilu_.n_up; ++l) {
+    const int n = up_off_h_[l + 1] - up_off_h_[l];
+    k_ilu_upper<<<(n + 127) / 128, 128, 0, s>>>(ilu_.up_cells + up_off_h_[l], n, ilu_, z, z, gate);
+  }
 }
 
 Work<double> Solver::alloc_work() {
@@ -386,9 +551,9 @@ void Solver::state_get(double* U_ref) { to_reference(U_, U_ref); }
 
 void Solver::state_freestream() {
   // init_one_x (src/init.cpp:57-81) == the freestream boundary state.
-  std::vector<Vec4<double>> u(hm_.nc, Vec4<double>{phys_.fs_rho, phys_.fs_rhou, phys_.fs_rhov, phys_.fs_E});
-  O2F_CUDA(cudaMemcpyAsync(U_, u.data(), u.size() * sizeof(Vec4<double>), cudaMemcpyHostToDevice, stream_));
-  sync();
+  k_fill_state<double><<<grid(topo_.nc), kBlock, 0, stream_>>>(
+      topo_.nc, Vec4<double>{phys_.fs_rho, phys_.fs_rhou, phys_.fs_rhov, phys_.fs_E}, U_);
+  O2F_CUDA(cudaGetLastError());
   have_residual_ = false;
   blk_valid_ = false;
 }
@@ -435,6 +600,62 @@ void Solver::residual(double* R_ref) {
   have_residual_ = true;
   blk_valid_ = false;
   if (R_ref) to_reference(work_.R, R_ref);
+}
+
+void Solver::profile_kernels(int reps, double* ms_out) {
+  if (reps <= 0) throw Error(O2F_ERR_ARG, "reps must be positive");
+  const Topo& t = topo_;
+  const Geom<double>& g = geom_;
+  const Work<double>& w = work_;
+  cudaStream_t s = stream_;
+  launch_residual(geom_, work_, U_, nullptr, false, nullptr);  // fresh interface states
+  have_residual_ = true;
+  blk_valid_ = false;
+  build_jt_blocks();
+  if (!tmp_) tmp_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  if (!s_) s_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  O2F_CUDA(cudaMemsetAsync(s_, 0, topo_.nc * sizeof(Vec4<double>), s));
+  for (int k = 0; k < O2F_K_COUNT; ++k) {
+    O2F_CUDA(cudaEventRecord(ev0_, s));
+    for (int r = 0; r < reps; ++r) {
+      switch (k) {
+        case O2F_K_VERTEX_STATE:
+          k_vertex_state<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, U_, phys_, w.vq,
+                                                               nullptr);
+          break;
+        case O2F_K_CELL_GRADIENT:
+          k_cell_gradient<double, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U_, w.vq,
+                                                                       phys_, w.eL, w.eR, w.ctq, w.ctqy, w.grad,
+                                                                       nullptr);
+          break;
+        case O2F_K_VERTEX_VISC:
+          k_vertex_visc<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, w.ctq, w.ctqy, w.vtq,
+                                                              w.vtqy, nullptr);
+          break;
+        case O2F_K_EDGE_FLUX:
+          k_edge_flux<double><<<grid(t.ne), kBlock, 0, s>>>(t.ne, g, t.ev, t.ebc, w.eL, w.eR, w.vtq, w.vtqy, phys_,
+                                                            w.F, w.etq, w.etqy, nullptr);
+          break;
+        case O2F_K_CELL_RESIDUAL:
+          k_cell_residual<double, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, w.F, w.etq, w.etqy, U_,
+                                                                       Uold_, w.R, RkStage{}, nullptr);
+          break;
+        case O2F_K_JT_APPLY:
+          jt_apply_dev(s_, tmp_);
+          break;
+        case O2F_K_JT_BLOCKS:
+          k_jt_blocks<<<(int)((t.ne + 127) / 128), 128, 0, s>>>(t.ne, g, t.ebc, w.eL, w.eR, phys_, 1e-6, blk_);
+          break;
+      }
+    }
+    O2F_CUDA(cudaEventRecord(ev1_, s));
+    O2F_CUDA(cudaGetLastError());
+    sync();
+    float ms = 0.f;
+    O2F_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    ms_out[k] = (double)ms / reps;
+  }
+  launches_ += (int64_t)reps * O2F_K_COUNT;
 }
 
 void Solver::debug_get(const std::string& which, double* out) {
@@ -640,22 +861,37 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   ks.tol2 = tol * tol * bb[0];
   int64_t total = 0;
   double relres = INFINITY;
-  const int kItersPerGraph = 8;
+  // Right-preconditioned BiCGSTAB: phat = M^{-1} p, shat = M^{-1} s; the
+  // recurrence residual r stays the true residual of J^T lambda = b.
+  const bool precond = params_.adjoint_precond == O2F_PRECOND_ILU0;
+  Vec4<double>* ph = p_;
+  Vec4<double>* sh = s_;
+  if (precond) {
+    ilu_factor();
+    ph = phat_;
+    sh = shat_;
+  }
+  const int kItersPerGraph = precond ? 1 : 8;
+  const int kernels_per_iter = 5 + (precond ? 2 * (ilu_.n_lo + ilu_.n_up) : 0);
+  const int* kgate = &ks_->stop;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   O2F_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
   for (int i = 0; i < kItersPerGraph; ++i) {
     k_bicg_p<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_),
                                                reinterpret_cast<double*>(p_), reinterpret_cast<double*>(v_), ks_);
-    k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, p_, v_, r0_,
+    if (precond) ilu_apply(p_, ph, kgate);
+    k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ph, v_, r0_,
                                                   part_, ks_);
     k_bicg_s<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(v_),
                                                reinterpret_cast<double*>(s_), ks_);
-    k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, s_, t_, part_,
-                                                  ks_);
-    k_bicg_xr<<<kRedGrid, kBlock, 0, stream_>>>(n4, x, reinterpret_cast<double*>(p_), reinterpret_cast<double*>(s_),
-                                                reinterpret_cast<double*>(t_), reinterpret_cast<double*>(r_),
-                                                reinterpret_cast<double*>(r0_), part_, ks_);
+    if (precond) ilu_apply(s_, sh, kgate);
+    k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, sh, s_, t_,
+                                                  part_, ks_);
+    k_bicg_xr<<<kRedGrid, kBlock, 0, stream_>>>(n4, x, reinterpret_cast<double*>(ph), reinterpret_cast<double*>(sh),
+                                                reinterpret_cast<double*>(s_), reinterpret_cast<double*>(t_),
+                                                reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_), part_,
+                                                ks_);
   }
   O2F_CUDA(cudaStreamEndCapture(stream_, &graph));
   O2F_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -686,7 +922,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
           const int reps = launched < 64 ? 1 : 4;
           for (int r = 0; r < reps; ++r) O2F_CUDA(cudaGraphLaunch(exec, stream_));
           launched += reps * kItersPerGraph;
-          launches_ += reps * kItersPerGraph * 5;
+          launches_ += (int64_t)reps * kItersPerGraph * kernels_per_iter;
         }
         const int64_t chunk_its = hks->it_chunk;
         total += chunk_its;
@@ -699,6 +935,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
         O2F_CUDA(cudaMemcpyAsync(hks, ks_, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream_));
         sync();
         relres = std::sqrt(hks->rr) / (bnorm > 0 ? bnorm : 1.0);
+        if (params_.verbosity >= 1) std::fprintf(stderr, "[adjoint] iters=%lld  relres=%g\n", (long long)total, relres);
         if (relres <= tol) break;
         if (!std::isfinite(relres)) {
           err = O2F_ERR_NONFINITE;

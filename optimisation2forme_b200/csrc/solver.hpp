@@ -68,6 +68,7 @@ class Solver {
   void shape_gradient(const o2f_shape_params& sp, const int* ids, int n, double beta, double eps,
                       const double* lambda_ref, double* grad);
   void debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which, double* out);
+  void profile_kernels(int reps, double* ms_out);
   double last_residual_ms() const { return last_residual_ms_; }
   int64_t launches() const { return launches_; }
 
@@ -115,6 +116,16 @@ class Solver {
   double* part_ = nullptr;
   unsigned int* ticket_ = nullptr;
   double* scal_ = nullptr;  // small device scalars
+  // block ILU(0) preconditioner of the adjoint
+  void setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector<int2>& ec,
+                      const std::vector<uint8_t>& ebc);
+  void ilu_factor();
+  void ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate);
+  std::vector<int32_t> ilu_nbr_h_, ilu_pos_h_, lo_off_h_, lo_cells_h_, up_off_h_, up_cells_h_;
+  IluDev ilu_{};
+  bool ilu_alloc_ = false;
+  int* ilu_status_ = nullptr;
+  Vec4<double>*phat_ = nullptr, *shat_ = nullptr;
   // shape perturbation
   Geom<double> pgeom_{};
   Work<double> pwork_{};

@@ -55,6 +55,7 @@ class SimulationParams:
     limiter_k: float = 1e-2
     limiter: str = "venkatakrishnan"
     precision: str = "fp64"
+    adjoint_precond: str = "ilu0"
     max_steps: int = 2**62
     residual_drop: float = 0.0
     adjoint_tol: float = 1e-6
@@ -75,6 +76,8 @@ class SimulationParams:
         else:
             raise ValueError(f"unknown limiter {self.limiter!r}")
         p.precision = {"fp64": _lib.PREC_F64, "fp32": _lib.PREC_F32}[self.precision.lower()]
+        p.adjoint_precond = {"none": 0, "identity": 0, "ilu0": 1}[self.adjoint_precond.lower()]
+        p.verbosity = int(self.verbosity)
         return p
 
 
@@ -82,7 +85,7 @@ _FLOAT_KEYS = {"cfl_number", "final_time", "gamma", "viscosity", "Pr", "cp", "in
                "aoa_deg", "limiter_k", "residual_drop", "adjoint_tol"}
 _INT_KEYS = {"verbosity", "max_steps", "adjoint_restart", "adjoint_max_iter"}
 _STR_KEYS = {"mesh_name", "boundary_conditions", "initial_condition", "state_load_path", "state_save_path",
-             "shape_param_file", "shape_log_file", "limiter", "precision"}
+             "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond"}
 
 
 def load_config(path: str | os.PathLike, params: SimulationParams | None = None) -> SimulationParams:
@@ -409,6 +412,13 @@ class Solver:
         check(lib().o2f_debug_perturbed(self._h, C.byref(shape), self.param_ids([name])[0], float(eps),
                                         which.encode(), _ptr(out)))
         return out
+
+    def profile_kernels(self, reps: int = 20) -> dict:
+        """Mean duration (ms) of one launch of each kernel class, CUDA events
+        on the context stream."""
+        ms = np.zeros(len(_lib.KERNEL_CLASSES))
+        check(lib().o2f_profile_kernels(self._h, int(reps), _ptr(ms)))
+        return dict(zip(_lib.KERNEL_CLASSES, ms.tolist()))
 
     def timing(self) -> dict:
         t = _lib.Timing()

@@ -1,0 +1,73 @@
+"""Failure detection on the GPU without a GPU fault: every error is a status
+returned to the host, caused by host-made inputs (a NaN state, an iteration
+cap, a call out of order).  No kernel traps or hangs: the device-driven loops
+carry step / iteration caps and stop flags that the host reads."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import desc_of, perturbed_freestream, small_mesh
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver():
+    from optimisation2forme_b200 import SimulationParams, Solver
+    m = small_mesh(triangles=True, n_surface=48, n_layers=12, seed=0)
+    p = SimulationParams(viscosity=1.8e-5, inflow_velocity=0.6, limiter_k=5.0, final_time=1.0, cfl_number=0.5,
+                         verbosity=0)
+    return Solver(p, desc=desc_of(m)), p
+
+
+def test_nonfinite_state_stops_the_time_loop_with_a_status():
+    from optimisation2forme_b200 import O2FError
+    s, p = _solver()
+    with s:
+        U = perturbed_freestream(s.n_cells, p, seed=1, amp=1e-3)
+        U[4 * 7] = np.nan
+        s.set_state(U)
+        with pytest.raises(O2FError) as e:
+            s.time_loop(50)
+        assert e.value.status == "O2F_ERR_NONFINITE"
+        # the context stays usable
+        s.initialize_freestream()
+        assert s.time_loop(3)["steps"] == 3
+
+
+def test_negative_density_is_reported_not_trapped():
+    from optimisation2forme_b200 import O2FError
+    s, p = _solver()
+    with s:
+        U = perturbed_freestream(s.n_cells, p, seed=1, amp=1e-3)
+        U[4 * 3] = -1.0
+        s.set_state(U)
+        with pytest.raises(O2FError) as e:
+            s.time_loop(200)
+        assert e.value.status == "O2F_ERR_NONFINITE"
+
+
+def test_adjoint_iteration_cap_returns_not_converged():
+    s, p = _solver()
+    with s:
+        s.initialize_freestream()
+        s.time_loop(50)
+        s.compute_residual()
+        res = s.solve_adjoint_system(beta=0.1, tol=1e-15, max_iter=3, restart=2, raise_on_failure=False)
+        assert res["status"] == "O2F_ERR_NOT_CONVERGED"
+        assert res["iters"] == 3
+        assert np.isfinite(res["relres"])
+
+
+def test_call_order_is_checked():
+    from optimisation2forme_b200 import O2FError
+    s, p = _solver()
+    with s:
+        with pytest.raises(O2FError) as e:
+            s.lift_drag()
+        assert e.value.status == "O2F_ERR_STATE"
+        with pytest.raises(O2FError) as e:
+            s.solve_adjoint_system()
+        assert e.value.status == "O2F_ERR_STATE"
+        with pytest.raises(ValueError):
+            s.set_state(np.zeros(5))

@@ -32,6 +32,32 @@ def build() -> bool:
     return False
 
 
+def write_binary_mesh(path: Path, mesh: dict) -> Path:
+    """The binary model variant read by oracle/shims/gmsh.h: the same groups
+    as meshgen.write_msh2 (FreeStream 1, Airfoil 2, Fluid 3), same orders."""
+    xy = np.asarray(mesh["node_xy"], dtype=np.float64).reshape(-1, 2)
+    seg = np.asarray(mesh["segments"], dtype=np.int64).reshape(-1, 2)
+    bc = np.asarray(mesh["segment_bc"])
+    offs = np.asarray(mesh["cell_offsets"], dtype=np.int64)
+    cn = np.asarray(mesh["cell_nodes"], dtype=np.int64)
+    sizes = np.diff(offs)
+    with open(path, "wb") as fh:
+        fh.write(b"O2FMSHB1")
+        fh.write(np.int64(len(xy)).tobytes())
+        fh.write(np.concatenate([xy, np.zeros((len(xy), 1))], axis=1).astype("<f8").tobytes())
+        names = [(1, 1, b"FreeStream"), (1, 2, b"Airfoil"), (2, 3, b"Fluid")]
+        fh.write(np.int64(len(names)).tobytes())
+        for d, t, n in names:
+            fh.write(np.array([d, t, len(n)], dtype="<i4").tobytes() + n)
+        fh.write(np.int64(len(seg) + len(sizes)).tobytes())
+        tag = np.where(bc == ord("f"), 1, 2)
+        hdr_seg = np.stack([np.ones(len(seg), dtype=np.int64), tag, tag], axis=1)
+        hdr_cell = np.stack([np.where(sizes == 3, 2, 3), np.full(len(sizes), 3), np.full(len(sizes), 3)], axis=1)
+        fh.write(np.concatenate([hdr_seg, hdr_cell]).astype("<i4").tobytes())
+        fh.write((np.concatenate([seg.reshape(-1), cn]) + 1).astype("<i8").tobytes())
+    return Path(path)
+
+
 def write_config(path: Path, *, mesh: str, state: str = "", params_file: str = "", viscosity=1.8e-5,
                  inflow_velocity=0.3, cfl=0.5, final_time=0.005, Pr=0.71, extra: str = "") -> Path:
     """A reference config file (keys of src/params.cpp:35-77)."""

@@ -323,18 +323,29 @@ int main(int argc, char** argv) {
     } else if (mode == "march") {
       march(mesh, params, std::atoi(argv[4]));
     } else if (mode == "bench") {
+      // Per-call wall times of the reference's computeResidual and
+      // applyJacobianTranspose, `reps` samples each (the first residual call
+      // sizes the static scratch buffers and is not timed).
       const int reps = std::max(1, std::atoi(argv[4]));
-      residual(mesh, params);  // first call sizes the static scratch buffers
-      double t0 = now_s();
-      for (int r = 0; r < reps; ++r) residual(mesh, params);
-      double t_res = (now_s() - t0) / reps;
+      residual(mesh, params);
+      std::vector<double> t_res, t_jt;
+      for (int r = 0; r < reps; ++r) {
+        double t0 = now_s();
+        residual(mesh, params);
+        t_res.push_back(now_s() - t0);
+      }
       std::vector<double> x(nc, 1e-3), y0(nc), y1(nc), y2(nc), y3(nc);
-      applyJacobianTranspose(mesh, params, x, x, x, x, y0, y1, y2, y3, 1e-6);
-      t0 = now_s();
-      for (int r = 0; r < reps; ++r) applyJacobianTranspose(mesh, params, x, x, x, x, y0, y1, y2, y3, 1e-6);
-      double t_jt = (now_s() - t0) / reps;
-      std::printf("{\"cells\": %zu, \"edges\": %zu, \"threads\": %d, \"residual_s\": %.9g, \"jt_s\": %.9g}\n",
-                  nc, mesh.edges.size(), omp_get_max_threads(), t_res, t_jt);
+      for (int r = 0; r < reps; ++r) {
+        double t0 = now_s();
+        applyJacobianTranspose(mesh, params, x, x, x, x, y0, y1, y2, y3, 1e-6);
+        t_jt.push_back(now_s() - t0);
+      }
+      std::printf("{\"cells\": %zu, \"edges\": %zu, \"threads\": %d, \"residual_s\": [", nc, mesh.edges.size(),
+                  omp_get_max_threads());
+      for (int r = 0; r < reps; ++r) std::printf("%s%.9g", r ? ", " : "", t_res[r]);
+      std::printf("], \"jt_s\": [");
+      for (int r = 0; r < reps; ++r) std::printf("%s%.9g", r ? ", " : "", t_jt[r]);
+      std::printf("]}\n");
     } else {
       throw std::runtime_error("unknown mode " + mode);
     }

@@ -75,10 +75,57 @@ namespace option {
 inline void setNumber(const std::string&, const double) {}
 }  // namespace option
 
+// Binary variant of the same model, written by oracle/ref.py for large
+// meshes: "O2FMSHB1", int64 n_nodes, n_nodes x (x,y,z) f64 (tags 1..n),
+// int64 n_names, per name (int32 dim, int32 tag, int32 len, bytes), int64
+// n_elements, int32 type/phys/entity per element, then the int64 node tags.
+inline bool open_binary(const std::string& fileName) {
+  using namespace detail;
+  std::ifstream in(fileName, std::ios::binary);
+  char magic[8] = {0};
+  if (!in.read(magic, 8) || std::string(magic, 8) != "O2FMSHB1") return false;
+  Model& m = state();
+  int64_t n = 0;
+  in.read(reinterpret_cast<char*>(&n), 8);
+  std::vector<double> xyz(3 * n);
+  in.read(reinterpret_cast<char*>(xyz.data()), 24 * n);
+  for (int64_t i = 0; i < n; ++i) m.nodes[i + 1] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+  int64_t nn = 0;
+  in.read(reinterpret_cast<char*>(&nn), 8);
+  for (int64_t i = 0; i < nn; ++i) {
+    int32_t d[3];
+    in.read(reinterpret_cast<char*>(d), 12);
+    std::string name(d[2], '\0');
+    in.read(&name[0], d[2]);
+    m.names[{d[0], d[1]}] = name;
+  }
+  int64_t ne = 0;
+  in.read(reinterpret_cast<char*>(&ne), 8);
+  std::vector<int32_t> hdr(3 * ne);
+  in.read(reinterpret_cast<char*>(hdr.data()), 12 * ne);
+  int64_t total = 0;
+  for (int64_t i = 0; i < ne; ++i) total += element_nodes(hdr[3 * i]);
+  std::vector<int64_t> tags(total);
+  in.read(reinterpret_cast<char*>(tags.data()), 8 * total);
+  if (!in) throw std::runtime_error("gmsh shim: truncated binary mesh " + fileName);
+  m.elements.resize(ne);
+  int64_t o = 0;
+  for (int64_t i = 0; i < ne; ++i) {
+    Element& e = m.elements[i];
+    e.type = hdr[3 * i];
+    e.phys = hdr[3 * i + 1];
+    e.entity = hdr[3 * i + 2];
+    e.nodes.assign(tags.begin() + o, tags.begin() + o + element_nodes(e.type));
+    o += element_nodes(e.type);
+  }
+  return true;
+}
+
 inline void open(const std::string& fileName) {
   using namespace detail;
   Model& m = state();
   m = Model();
+  if (open_binary(fileName)) return;
   std::ifstream in(fileName);
   if (!in) throw std::runtime_error("gmsh shim: cannot open " + fileName);
   std::string line;

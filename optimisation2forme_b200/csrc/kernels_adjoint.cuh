@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(kBlock) k_wave_speed(int64_t nc, const Vec4<T>
                                                        StepState* st) {
   if (st->stop) return;
   double m = 0.0;
+  bool bad = false;  // a non-finite speed anywhere stops the loop
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
     const Vec4<T> q = U[c];
     const double rho = q.a, ru = q.b, rv = q.c, E = q.d;
@@ -105,14 +106,16 @@ __global__ void __launch_bounds__(kBlock) k_wave_speed(int64_t nc, const Vec4<T>
     const double p = (gamma - 1.0) * (E - kinetic);
     const double cs = sqrt(gamma * p / rho);
     const double speed = hypot(u, v) + cs;
-    if (!(speed <= m)) m = speed;  // NaN propagates
+    if (!(speed <= 1.7976931348623157e308)) bad = true;  // NaN or +inf
+    else if (speed > m) m = speed;
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double other = __shfl_down_sync(0xffffffffu, m, o);
-    if (!(other <= m)) m = other;
+    if (other > m) m = other;
   }
+  bad = __any_sync(0xffffffffu, bad);
   if ((threadIdx.x & 31) == 0) {
-    if (m != m) {
+    if (bad) {
       atomicExch(&st->stop, 2);
     } else if (m > 0.0) {
       atomicMax(&st->max_wave_bits, (unsigned long long)__double_as_longlong(m));
@@ -144,7 +147,7 @@ __global__ void k_step_norm(const double* part, int nparts, double* hist, StepSt
     const double nrm = sqrt(tot);
     if (hist) hist[st->step] = nrm;
     if (st->step == 0) st->hist0 = nrm;
-    if (!(nrm == nrm)) st->stop = 2;
+    if (!(nrm <= 1.7976931348623157e308)) st->stop = 2;  // NaN or +inf
     if (st->drop_tol > 0.0 && st->hist0 > 0.0 && nrm <= st->drop_tol * st->hist0) st->drop_hit = 1;
   }
 }

@@ -21,14 +21,15 @@ import numpy as np
 
 
 def naca4_surface(m: float, p: float, t: float, n: int, chord: float = 1.0, pos_x: float = 0.355,
-                  n_te: int = 2) -> np.ndarray:
+                  n_te: int = 3, cluster: float = 1.0) -> np.ndarray:
     """Closed surface loop, counter-clockwise from the upper trailing edge over
     the leading edge to the lower trailing edge, then across the blunt base.
     Camber/thickness: the yc/yt formulas of the reference
-    (src/shape_optimization.cpp:807-826)."""
+    (src/shape_optimization.cpp:807-826).  ``cluster`` blends cosine
+    clustering (1) with uniform spacing (0) along the chord."""
     k = n // 2
-    beta = np.linspace(0.0, math.pi, k + 1)
-    xr = 0.5 * (1.0 - np.cos(beta))  # 0 .. 1, clustered at both ends
+    s = np.linspace(0.0, 1.0, k + 1)
+    xr = cluster * 0.5 * (1.0 - np.cos(math.pi * s)) + (1.0 - cluster) * s  # 0 .. 1
 
     def yc(x):
         if m == 0.0:
@@ -67,6 +68,7 @@ class OGridSpec:
     pos_x: float = 0.355
     chord: float = 1.0
     jitter: float = 0.1
+    cluster: float = 1.0
 
 
 def _normals(S: np.ndarray) -> np.ndarray:
@@ -86,7 +88,7 @@ def naca_ogrid(spec: OGridSpec):
     """Returns dict(node_xy, segments, segment_bc, cell_offsets, cell_nodes):
     an o2f mesh description in construction order."""
     rng = np.random.default_rng(spec.seed)
-    S = naca4_surface(spec.m, spec.p, spec.t, spec.n_surface, spec.chord, spec.pos_x)
+    S = naca4_surface(spec.m, spec.p, spec.t, spec.n_surface, spec.chord, spec.pos_x, cluster=spec.cluster)
     # The loop runs TE(upper) -> LE -> TE(lower) -> base: counter-clockwise,
     # so the outward normals are (dy, -dx).
     ni = S.shape[0]
@@ -130,9 +132,15 @@ def naca_ogrid(spec: OGridSpec):
             # (a, b, c, dd) runs clockwise (i counter-clockwise along the
             # surface, j outward); cells are stored counter-clockwise.
             a, b, c, dd = vid[j, i], vid[j, i1], vid[j + 1, i1], vid[j + 1, i]
+            # In the first and last layers the diagonals alternate, so every
+            # wall and far-field vertex has 2 or 4 cells: 3 cells would make
+            # the reference's barycentric vertex weights extrapolate from the
+            # thin triangle of cell centres (weights far outside [0, 1]).
+            edge_layer = j == 0 or j == nl - 1
+            split_ac = (i % 2 == 0) if edge_layer else rng.random() < 0.5
             if not spec.triangles:
                 cells.append((a, dd, c, b))
-            elif rng.random() < 0.5:
+            elif split_ac:
                 cells.append((a, c, b))
                 cells.append((a, dd, c))
             else:

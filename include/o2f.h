@@ -70,6 +70,15 @@ typedef enum o2f_status {
 #define O2F_PRECOND_NONE 0
 #define O2F_PRECOND_ILU0 1
 
+/* Diffusive time-step bound.  REFERENCE is 0.5*min_h^2/mu
+ * (src/simulation.cpp:109).  THERMAL uses 0.5*min_h^2/max(mu, kappa*(gamma-1)):
+ * the reference's heat flux q = -kappa*grad((gamma-1)*e) has no 1/R factor
+ * (src/diffusion.cpp:237-240), so its effective diffusivity is kappa*(gamma-1),
+ * which the reference's bound ignores; on cells below ~1e-5 chord that term
+ * is the explicit stability limit.  The residual is the same in both modes. */
+#define O2F_DT_REFERENCE 0
+#define O2F_DT_THERMAL 1
+
 /* Arithmetic of the residual / Jacobian-transpose kernels. */
 #define O2F_PREC_F64 0 /* FP64 throughout (parity mode)                           */
 #define O2F_PREC_F32 1 /* FP32 residual and JT, FP64 reductions, dt and Krylov     */
@@ -94,7 +103,8 @@ typedef struct o2f_params {
   int limiter;            /* NEW: O2F_LIMITER_*                                */
   int precision;          /* NEW: O2F_PREC_*                                   */
   int adjoint_precond;    /* NEW: O2F_PRECOND_* (default ILU0)                 */
-  int verbosity;          /* >= 1: "[adjoint] iters=.. relres=.." per restart chunk
+  int dt_mode;            /* NEW: O2F_DT_* diffusive time-step bound             */
+  int verbosity;        /* >= 1: "[adjoint] iters=.. relres=.." per restart chunk
                              on stderr, as src/shape_optimization.cpp:719 prints */
 } o2f_params;
 

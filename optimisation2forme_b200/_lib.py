@@ -54,6 +54,7 @@ class Params(C.Structure):
         ("limiter", C.c_int),
         ("precision", C.c_int),
         ("adjoint_precond", C.c_int),
+        ("dt_mode", C.c_int),
         ("verbosity", C.c_int),
     ]
 

@@ -91,6 +91,7 @@ void o2f_params_default(o2f_params* p) {
   p->limiter = O2F_LIMITER_VENKAT;
   p->precision = O2F_PREC_F64;
   p->adjoint_precond = O2F_PRECOND_ILU0;
+  p->dt_mode = O2F_DT_REFERENCE;
   p->verbosity = 0;
 }
 

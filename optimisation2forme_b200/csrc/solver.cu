@@ -46,6 +46,7 @@ void validate_params(const o2f_params& p) {
   if (p.precision != O2F_PREC_F64) throw Error(O2F_ERR_ARG, "this context supports O2F_PREC_F64");
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
+  if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
 }
 
 }  // namespace
@@ -724,6 +725,8 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
   st.cfl = params_.cfl_number;
   st.min_h = min_h_;
   st.mu = params_.viscosity;
+  if (params_.dt_mode == O2F_DT_THERMAL)
+    st.mu = std::max(params_.viscosity, params_.viscosity * params_.cp / params_.Pr * (params_.gamma - 1.0));
   st.drop_tol = drop_tol;
   st.max_steps = max_steps;
   O2F_CUDA(cudaMemcpyAsync(step_, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));

@@ -93,24 +93,36 @@ def naca_ogrid(spec: OGridSpec):
     # so the outward normals are (dy, -dx).
     ni = S.shape[0]
     N = _normals(S)
-    # Radial distances: geometric boundary layer, then geometric blend to the far field.
+    # Radial distances: one smooth sequence of layer spacings -- geometric
+    # growth from the first cell until the cells are about isotropic (mean
+    # tangential spacing), then a geometric ratio solved so that the last
+    # layer lands on the far field.
     nl = spec.n_layers
-    d = [0.0]
-    h = spec.first_height
     chord = spec.chord
     centre = np.array([spec.pos_x + 0.5 * chord, 0.0])
-    while len(d) <= nl and d[-1] < 0.02 * chord and len(d) < nl // 3:
+    h_iso = 2.05 * chord / max(ni // 2, 1)
+    d = [0.0]
+    h = spec.first_height
+    while h < h_iso and len(d) < nl // 2:
         d.append(d[-1] + h)
         h *= spec.growth
     j1 = len(d) - 1
     rest = nl - j1
-    # the blend parameter f in [0, 1] grows geometrically from the boundary-layer edge
-    if rest > 0:
-        q = (spec.r_far / max(d[-1], 1e-12)) ** (1.0 / rest)
-        f = (np.power(q, np.arange(1, rest + 1)) - 1.0) / (q ** rest - 1.0)
+    span = spec.r_far - d[-1]
+    lo, hi = 1.0 + 1e-12, 4.0
+    if h * rest >= span:
+        q = 1.0 + 1e-12
     else:
-        f = np.zeros(0)
-    A = S + d[-1] * N  # edge of the boundary layer
+        for _ in range(200):  # h (q^rest - 1) / (q - 1) = span
+            q = 0.5 * (lo + hi)
+            if h * (q ** rest - 1.0) / (q - 1.0) > span:
+                hi = q
+            else:
+                lo = q
+    steps = h * np.power(q, np.arange(rest))
+    dist = np.cumsum(steps)
+    f = dist / dist[-1] if rest > 0 else np.zeros(0)
+    A = S + d[-1] * N  # edge of the wall-layer region
     theta = np.arctan2(A[:, 1] - centre[1], A[:, 0] - centre[0])
     F = centre + spec.r_far * np.stack([np.cos(theta), np.sin(theta)], axis=1)
     layers = [S + dj * N for dj in d]

@@ -56,6 +56,7 @@ class SimulationParams:
     limiter: str = "venkatakrishnan"
     precision: str = "fp64"
     adjoint_precond: str = "ilu0"
+    dt_mode: str = "reference"
     max_steps: int = 2**62
     residual_drop: float = 0.0
     adjoint_tol: float = 1e-6
@@ -77,6 +78,7 @@ class SimulationParams:
             raise ValueError(f"unknown limiter {self.limiter!r}")
         p.precision = {"fp64": _lib.PREC_F64, "fp32": _lib.PREC_F32}[self.precision.lower()]
         p.adjoint_precond = {"none": 0, "identity": 0, "ilu0": 1}[self.adjoint_precond.lower()]
+        p.dt_mode = {"reference": 0, "thermal": 1}[self.dt_mode.lower()]
         p.verbosity = int(self.verbosity)
         return p
 
@@ -85,7 +87,7 @@ _FLOAT_KEYS = {"cfl_number", "final_time", "gamma", "viscosity", "Pr", "cp", "in
                "aoa_deg", "limiter_k", "residual_drop", "adjoint_tol"}
 _INT_KEYS = {"verbosity", "max_steps", "adjoint_restart", "adjoint_max_iter"}
 _STR_KEYS = {"mesh_name", "boundary_conditions", "initial_condition", "state_load_path", "state_save_path",
-             "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond"}
+             "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond", "dt_mode"}
 
 
 def load_config(path: str | os.PathLike, params: SimulationParams | None = None) -> SimulationParams:
@@ -317,14 +319,19 @@ class Solver:
         check(lib().o2f_debug_get(self._h, name.encode(), _ptr(out)))
         return out
 
-    def time_loop(self, max_steps: int, residual_drop: float = 0.0) -> dict:
-        """Simulator::time_loop (src/simulation.cpp:68-126)."""
+    def time_loop(self, max_steps: int, residual_drop: float = 0.0, raise_on_failure: bool = True) -> dict:
+        """Simulator::time_loop (src/simulation.cpp:68-126).  On a non-finite
+        state the loop stops; with raise_on_failure=False the steps done and
+        the history up to that point are returned with the status."""
         hist = np.zeros(max(int(max_steps), 1))
         steps = C.c_int64()
         t = C.c_double()
-        check(lib().o2f_rk3_run(self._h, int(max_steps), float(residual_drop), _ptr(hist), C.byref(steps),
-                                C.byref(t)))
-        return {"steps": steps.value, "t": t.value, "history": hist[: min(steps.value, hist.size)]}
+        code = lib().o2f_rk3_run(self._h, int(max_steps), float(residual_drop), _ptr(hist), C.byref(steps),
+                                 C.byref(t))
+        if raise_on_failure:
+            check(code)
+        return {"steps": steps.value, "t": t.value, "history": hist[: min(steps.value, hist.size)],
+                "status": _lib.STATUS.get(code, "OK")}
 
     def lift_drag(self, beta: float = 1.0) -> tuple[float, float, float]:
         """(C_L, C_D, J): computeLiftDragCoefficients (src/compute.cpp:92-132)

@@ -31,7 +31,7 @@ class Params(C.Structure):
     _fields_ = [("gamma", C.c_double), ("viscosity", C.c_double), ("Pr", C.c_double), ("cp", C.c_double),
                 ("cfl_number", C.c_double), ("final_time", C.c_double), ("inflow_velocity", C.c_double),
                 ("rho_ref", C.c_double), ("p_ref", C.c_double), ("aoa_deg", C.c_double),
-                ("limiter_k", C.c_double), ("limiter", C.c_int)]
+                ("limiter_k", C.c_double), ("limiter", C.c_int), ("dt_mode", C.c_int)]
 
 
 class Shape(C.Structure):
@@ -100,7 +100,8 @@ class Oracle:
     def set_params(self, params) -> None:
         self.p = Params(params.gamma, params.viscosity, params.Pr, params.cp, params.cfl_number, params.final_time,
                         params.inflow_velocity, params.rho_ref, params.p_ref, params.aoa_deg, params.limiter_k,
-                        0 if params.limiter.lower() in ("venkatakrishnan", "venkat") else 1)
+                        0 if params.limiter.lower() in ("venkatakrishnan", "venkat") else 1,
+                        1 if params.dt_mode == "thermal" else 0)
 
     def residual(self, U):
         U = np.ascontiguousarray(U, dtype=np.float64)

@@ -519,7 +519,9 @@ int64_t o2fo_march(const o2fo_mesh* m, const o2fo_params* p, double* U, int64_t 
       max_wave = smax(max_wave, speed);
     }
     double dt_adv = p->cfl_number * min_h / max_wave;
-    double dt_diff = 0.5 * (min_h * min_h) / p->viscosity;
+    double mu_dt = p->viscosity;
+    if (p->dt_mode == 1) mu_dt = smax(p->viscosity, p->viscosity * p->cp / p->Pr * (p->gamma - 1.0));
+    double dt_diff = 0.5 * (min_h * min_h) / mu_dt;
     double dt = smin(dt_adv, dt_diff);
     memcpy(Uo, U, sizeof(double) * 4 * nc);
     static const double cs[3][2] = {{0.0, 1.0}, {3.0 / 4.0, 1.0 / 4.0}, {1.0 / 3.0, 2.0 / 3.0}};

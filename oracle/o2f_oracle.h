@@ -43,6 +43,7 @@ typedef struct o2fo_params {
   double gamma, viscosity, Pr, cp, cfl_number, final_time, inflow_velocity, rho_ref, p_ref;
   double aoa_deg, limiter_k;
   int limiter; /* 0 Venkatakrishnan, 1 Barth-Jespersen */
+  int dt_mode; /* 0 reference diffusive dt, 1 also bounded by kappa*(gamma-1) */
 } o2fo_params;
 
 typedef struct o2fo_shape {

@@ -1,11 +1,16 @@
 """Benchmark of the shape-gradient hot path (one JSON line on rank 0).
 
 One step = one shape-gradient evaluation: freestream start, SSP-RK3 time
-loop, lift/drag and J = -C_L + beta C_D, adjoint solve (BiCGSTAB, true
-relres <= tol), shape gradient dJ/d(m, p, t) by the perturbed-residual pairs.
+loop, lift/drag and J = -C_L + beta C_D, adjoint solve (BiCGSTAB to a true
+relres <= 1e-8 or the workload's iteration cap), shape gradient dJ/d(m, p, t)
+by the perturbed-residual pairs.
 Default workload ("large"): NACA 0012, seeded O-grid of ~2.0M triangles
 (first cell 1e-4 chord, growth 1.1), M = 0.85, AoA = 1.25 deg, FP64,
-20,000 SSP-RK3 steps, adjoint tol 1e-8.
+20,000 SSP-RK3 steps at CFL 0.3, then one 500-iteration BiCGSTAB restart
+chunk: on this mesh and impulsive-start state neither the reference's
+identity-preconditioned BiCGSTAB (it diverges) nor the block-ILU(0) one
+reaches 1e-8, so the evaluation does the reference's fixed chunk of work and
+the line reports the relres it reached.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl o2f|reference]
 
@@ -32,10 +37,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "shape-gradient evals/s (state+adjoint) vs plain FP64 GPU at dJ rel err≤1e-4"
-# Adjoint iterations of the workload with the block ILU(0) BiCGSTAB, measured
-# on the GPU path; the reference arm extrapolates with the same count (the
-# reference's identity-preconditioned solver needs far more).
-ADJOINT_ITERS = {"large": 400, "mixed": 400, "small": 350}
+# Adjoint iteration cap per evaluation (one restart chunk of the reference's
+# solver, src/shape_optimization.cpp:691) for the wall-refined workloads,
+# where BiCGSTAB does not reach 1e-8; "small" converges (about 350-550
+# iterations with block ILU(0)).  The reference arm extrapolates with the
+# iteration count of the GPU path (the cap, or 350 for "small").
+ADJOINT_CAP = {"large": 500, "mixed": 500, "small": 100000}
+ADJOINT_ITERS = {"large": 500, "mixed": 500, "small": 350}
 
 
 def load_peaks() -> dict:
@@ -51,14 +59,17 @@ def workload(name: str):
     from optimisation2forme_b200.meshgen import config_mesh, naca_ogrid
     spec, flow = config_mesh(name)
     mesh = naca_ogrid(spec)
-    if name == "small":
-        cfl, rk_steps = 0.5, 2000
-    else:
-        cfl, rk_steps = 0.1, 20000
+    # CFL / diffusive time-step bound / preconditioner shift per workload: the
+    # 1e-4-chord wall layers need the thermal dt bound and CFL <= 0.5 (0.3 on
+    # the 2M-cell mesh) for the reference scheme to stay finite over 20k steps.
+    cfl, rk_steps, dt_mode, shift = {"small": (0.5, 2000, "reference", 0.0),
+                                     "mixed": (0.5, 20000, "thermal", 0.2),
+                                     "large": (0.3, 20000, "thermal", 0.2)}[name]
     # Reference physics at the reference's own viscosity (mu = 1.8e-5): the
     # reference's viscous operator diverges at the configs' Reynolds numbers.
     params = SimulationParams(viscosity=1.8e-5, inflow_velocity=flow["mach"], aoa_deg=flow["aoa"], cfl_number=cfl,
-                              final_time=1e30, limiter_k=5.0, adjoint_precond="ilu0", verbosity=0)
+                              final_time=1e30, limiter_k=5.0, adjoint_precond="ilu0", adjoint_shift=shift,
+                              dt_mode=dt_mode, verbosity=0)
     shape = dict(m=spec.m, p=spec.p, t=spec.t, pos_x=spec.pos_x, c=spec.chord)
     return spec, flow, mesh, params, shape, rk_steps
 
@@ -151,10 +162,20 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
     beta = 0.1
     last = {}
 
+    cap = ADJOINT_CAP[args.workload]
+
+    def adjoint_and_gradient():
+        _, _, J = s.lift_drag(beta)
+        a = s.solve_adjoint_system(beta, tol=args.adjoint_tol, max_iter=cap, restart=500, raise_on_failure=False)
+        if a["status"] not in ("OK", "O2F_ERR_NOT_CONVERGED"):
+            raise RuntimeError(f"adjoint solve failed: {a['status']}")
+        g = s.compute_shape_gradient(names, sp, beta=beta, eps=1e-6)
+        return {"J": J, "iters": a["iters"], "relres": a["relres"], "grad": g}
+
     def evaluation():
         s.initialize_freestream()
         s.time_loop(rk_steps)
-        last.update(s.optimize_shape(names, sp, beta=beta, eps=1e-6, tol=args.adjoint_tol))
+        last.update(adjoint_and_gradient())
 
     def barrier():
         if world > 1:
@@ -194,7 +215,7 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
         for _ in range(args.e2e_steps):
             s.set_state(U0)
             s.time_loop(rk_steps)
-            s.optimize_shape(names, sp, beta=beta, eps=1e-6, tol=args.adjoint_tol)
+            adjoint_and_gradient()
             Uf = s.get_state()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
@@ -203,7 +224,7 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             dt = float(t.item())
         e2e = {"value": world * args.e2e_steps / dt, "unit": "evals/s", "h2d_bytes_per_step": int(U0.nbytes),
-               "d2h_bytes_per_step": int(Uf.nbytes + 8 * len(names) + 24)}
+               "d2h_bytes_per_step": int(Uf.nbytes + 8 * s.n_cells * 4 + 8 * len(names) + 24)}
 
     # Per-kernel launch durations (CUDA events on the solver's stream) about
     # the state the timed evaluations left.
@@ -232,7 +253,8 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
                                f"AoA={flow['aoa']:.2f}, {rk_steps} SSP-RK3 steps, adjoint tol {args.adjoint_tol}, "
                                "dJ/d(m,p,t)",
                    "cells": s.n_cells, "edges": s.n_edges, "rk_steps": rk_steps, "cfl": params.cfl_number,
-                   "viscosity": params.viscosity, "adjoint": "BiCGSTAB + block ILU(0)",
+                   "dt_mode": params.dt_mode, "viscosity": params.viscosity,
+                   "adjoint": f"BiCGSTAB + block ILU(0), shift {params.adjoint_shift}, cap {cap} iterations",
                    "adjoint_iters": last.get("iters"), "adjoint_relres": last.get("relres"), "J": last.get("J"),
                    "grad": [float(g) for g in last.get("grad", [])],
                    "l2": "inputs larger than L2 (working set > 126 MB)" if s.n_cells > 400000 else "working set fits L2",

@@ -100,6 +100,9 @@ typedef struct o2f_params {
   double aoa_deg;         /* NEW: angle of attack, rotates the freestream and
                              the lift/drag axes; 0 reproduces the reference    */
   double limiter_k;       /* NEW: Venkatakrishnan K, eps=(K h)^3; reference 1e-2 */
+  double adjoint_shift;   /* NEW: ILU(0) preconditioner built from J^T + s*|D_c| I
+                             (D_c: diagonal block, |.|: max row sum); 0 = plain
+                             ILU(0).  Changes the preconditioner only.          */
   int limiter;            /* NEW: O2F_LIMITER_*                                */
   int precision;          /* NEW: O2F_PREC_*                                   */
   int adjoint_precond;    /* NEW: O2F_PRECOND_* (default ILU0)                 */

@@ -51,6 +51,7 @@ class Params(C.Structure):
         ("p_ref", C.c_double),
         ("aoa_deg", C.c_double),
         ("limiter_k", C.c_double),
+        ("adjoint_shift", C.c_double),
         ("limiter", C.c_int),
         ("precision", C.c_int),
         ("adjoint_precond", C.c_int),

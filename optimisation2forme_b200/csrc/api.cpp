@@ -88,6 +88,7 @@ void o2f_params_default(o2f_params* p) {
   p->p_ref = 101325.0;
   p->aoa_deg = 0.0;
   p->limiter_k = 1e-2;  // k_eps of computeVenkatAlpha (src/advection.cpp:209)
+  p->adjoint_shift = 0.0;
   p->limiter = O2F_LIMITER_VENKAT;
   p->precision = O2F_PREC_F64;
   p->adjoint_precond = O2F_PRECOND_ILU0;

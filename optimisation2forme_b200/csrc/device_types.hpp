@@ -101,17 +101,28 @@ struct Phys {
 };
 
 // Block ILU(0) preconditioner of the adjoint operator (see ilu.cuh).
+// State of one sync-free triangular sweep (one per direction): warps take
+// 32-row chunks in ILU order from `claim`; the last warp to finish resets
+// claim/done and advances `epoch`, so a row is ready in the current launch
+// when its flag equals epoch + 1.
+struct SweepSync {
+  unsigned int claim;
+  unsigned int done;
+  unsigned int epoch;
+  int err;  // a dependency wait ran past its limit (the sweep's result is invalid)
+};
+
 struct IluDev {
   int64_t nc;
-  int32_t* nbr;     // [4*nc] neighbour cell of each slot (slot order = jslot order), -1 if none
-  int32_t* pos;     // [nc] position of the cell in the ILU order
-  double* A;        // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
-  double* Dinv;     // [nc*16]
-  int32_t* lo_off;  // [n_lo+1] forward levels
-  int32_t* lo_cells;
-  int32_t* up_off;  // [n_up+1] backward levels
-  int32_t* up_cells;
-  int n_lo, n_up;
+  int32_t* nbr;       // [4*nc] neighbour cell of each slot (slot order = jslot order), -1 if none
+  int32_t* pos;       // [nc] position of the cell in the ILU order
+  int32_t* order;     // [nc] cell at each ILU position (inverse of pos)
+  double* A;          // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
+  double* Dinv;       // [nc*16]
+  int32_t* lo_cells;  // [nc] factorization levels, concatenated (offsets kept on the host)
+  uint32_t* flag;     // [2*nc] ready flags of the forward, then the backward sweep
+  SweepSync* sync;    // [2] forward, backward
+  int n_lo;
 };
 
 // Buffers written by one residual evaluation.

@@ -91,7 +91,8 @@ __device__ __forceinline__ bool mat4_inv(const double* a_in, double* inv) {
 __global__ void __launch_bounds__(kBlock) k_ilu_assemble(int64_t nc, const int32_t* __restrict__ jslot, Geom<double> g,
                                                          const int2* __restrict__ ec,
                                                          const uint8_t* __restrict__ ebc,
-                                                         const double* __restrict__ blk, IluDev ilu) {
+                                                         const double* __restrict__ blk, double shift,
+                                                         IluDev ilu) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double* row = ilu.A + c * 80;
@@ -122,6 +123,14 @@ __global__ void __launch_bounds__(kBlock) k_ilu_assemble(int64_t nc, const int32
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int q = 0; q < 4; ++q) nb[r * 4 + q] = so * B[q * 4 + r];
+  }
+  if (shift > 0.0) {  // pseudo-time shift: s times the block's max row sum
+    double nrm = 0.0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      nrm = fmax(nrm, fabs(diag[r * 4]) + fabs(diag[r * 4 + 1]) + fabs(diag[r * 4 + 2]) + fabs(diag[r * 4 + 3]));
+#pragma unroll
+    for (int r = 0; r < 4; ++r) diag[r * 5] += (diag[r * 5] < 0.0 ? -shift : shift) * nrm;
   }
 #pragma unroll
   for (int i = 0; i < 16; ++i) row[i] = diag[i];
@@ -179,61 +188,124 @@ __global__ void __launch_bounds__(128) k_ilu_factor(const int32_t* __restrict__ 
   if (!mat4_inv(row, ilu.Dinv + (int64_t)i * 16)) atomicExch(status, 1);
 }
 
-// One forward level: y_i = r_i - sum_{k lower} L_ik y_k.
-__global__ void __launch_bounds__(128) k_ilu_lower(const int32_t* __restrict__ cells, int n, IluDev ilu,
-                                                   const Vec4<double>* __restrict__ r, Vec4<double>* __restrict__ y,
-                                                   const int* gate) {
-  if (gated(gate)) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int i = cells[t];
-  const int64_t nc = ilu.nc;
-  const int pi = ilu.pos[i];
-  const double* row = ilu.A + (int64_t)i * 80;
-  Vec4<double> acc = r[i];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int o = ilu.nbr[(int64_t)k * nc + i];
-    if (o < 0 || ilu.pos[o] > pi) continue;
-    const double* Lb = row + 16 * (1 + k);
-    const Vec4<double> v = y[o];
-    acc.a -= Lb[0] * v.a + Lb[1] * v.b + Lb[2] * v.c + Lb[3] * v.d;
-    acc.b -= Lb[4] * v.a + Lb[5] * v.b + Lb[6] * v.c + Lb[7] * v.d;
-    acc.c -= Lb[8] * v.a + Lb[9] * v.b + Lb[10] * v.c + Lb[11] * v.d;
-    acc.d -= Lb[12] * v.a + Lb[13] * v.b + Lb[14] * v.c + Lb[15] * v.d;
-  }
-  y[i] = acc;
+// Sync-free triangular sweeps (one launch per triangle).  Each warp takes
+// one 32-row chunk of the ILU order from a counter, so every chunk before it
+// already belongs to a running warp and the earliest unfinished row always
+// has its dependencies done: the waits cannot deadlock.  A row waits on the
+// ready flags of its lower (forward) or upper (backward) neighbours, solves
+// its 4-vector and releases its own flag.  Waits are bounded: past
+// kSweepSpinLimit polls the warp records sync->err and stops waiting, and
+// every other waiting row gives up once it sees the error.
+constexpr int kSweepBlock = 128;
+constexpr long long kSweepSpinLimit = 1ll << 22;
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
-// One backward level: z_i = D_i^{-1} (y_i - sum_{j upper} U_ij z_j); z may alias y.
-__global__ void __launch_bounds__(128) k_ilu_upper(const int32_t* __restrict__ cells, int n, IluDev ilu,
-                                                   const Vec4<double>* y, Vec4<double>* z, const int* gate) {
+__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ Vec4<double> ldcg4(const Vec4<double>* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 a = __ldcg(q), b = __ldcg(q + 1);
+  return Vec4<double>{a.x, a.y, b.x, b.y};
+}
+
+// kForward: y_i = r_i - sum_{k lower} L_ik y_k.
+// backward: z_i = D_i^{-1} (y_i - sum_{j upper} U_ij z_j), in place (y == z).
+template <bool kForward>
+__global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, const Vec4<double>* r,
+                                                           Vec4<double>* y, const int* gate) {
   if (gated(gate)) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int i = cells[t];
-  const int64_t nc = ilu.nc;
-  const int pi = ilu.pos[i];
-  const double* row = ilu.A + (int64_t)i * 80;
-  Vec4<double> acc = y[i];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int o = ilu.nbr[(int64_t)k * nc + i];
-    if (o < 0 || ilu.pos[o] < pi) continue;
-    const double* Ub = row + 16 * (1 + k);
-    const Vec4<double> v = z[o];
-    acc.a -= Ub[0] * v.a + Ub[1] * v.b + Ub[2] * v.c + Ub[3] * v.d;
-    acc.b -= Ub[4] * v.a + Ub[5] * v.b + Ub[6] * v.c + Ub[7] * v.d;
-    acc.c -= Ub[8] * v.a + Ub[9] * v.b + Ub[10] * v.c + Ub[11] * v.d;
-    acc.d -= Ub[12] * v.a + Ub[13] * v.b + Ub[14] * v.c + Ub[15] * v.d;
+  constexpr unsigned int kFull = 0xffffffffu;
+  SweepSync* sync = ilu.sync + (kForward ? 0 : 1);
+  unsigned int* flag = ilu.flag + (kForward ? 0 : ilu.nc);
+  const int lane = threadIdx.x & 31;
+  const unsigned int nchunks = (unsigned int)(n + 31) / 32u;
+  // Surplus warps of the last block leave before claiming: exactly nchunks
+  // claims per launch, so the reset below runs after the last claim.
+  if (blockIdx.x * (unsigned int)(kSweepBlock / 32) + (threadIdx.x >> 5) >= nchunks) return;
+  unsigned int chunk = 0, epoch = 0;
+  if (lane == 0) {
+    chunk = atomicAdd(&sync->claim, 1u);
+    epoch = *reinterpret_cast<volatile unsigned int*>(&sync->epoch);
   }
-  const double* D = ilu.Dinv + (int64_t)i * 16;
-  Vec4<double> out;
-  out.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
-  out.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
-  out.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
-  out.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
-  z[i] = out;
+  chunk = __shfl_sync(kFull, chunk, 0);
+  epoch = __shfl_sync(kFull, epoch, 0);
+  const unsigned int want = epoch + 1u;
+  const int64_t nc = ilu.nc;
+  const int p = (int)chunk * 32 + lane;
+  const bool active = p < n;
+  int i = 0, dep[4], ndep = 0, slot[4];
+  if (active) {
+    i = ilu.order[kForward ? p : n - 1 - p];
+    const int pi = ilu.pos[i];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int o = ilu.nbr[k * nc + i];
+      if (o < 0) continue;
+      const int po = ilu.pos[o];
+      if (kForward ? po < pi : po > pi) {
+        dep[ndep] = o;
+        slot[ndep] = k;
+        ++ndep;
+      }
+    }
+  }
+  bool done = !active;
+  long long spins = 0;
+  while (__any_sync(kFull, !done)) {
+    if (done) continue;
+    bool ready = true;
+    for (int d = 0; d < ndep; ++d)
+      if (ld_acquire_u32(flag + dep[d]) != want) ready = false;
+    if (ready) {
+      const double* row = ilu.A + (int64_t)i * 80;
+      Vec4<double> acc = kForward ? r[i] : ldcg4(y + i);
+      for (int d = 0; d < ndep; ++d) {
+        const double* Bk = row + 16 * (1 + slot[d]);
+        const Vec4<double> v = ldcg4(y + dep[d]);
+        acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
+        acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
+        acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
+        acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+      }
+      if (!kForward) {
+        const double* D = ilu.Dinv + (int64_t)i * 16;
+        Vec4<double> out;
+        out.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
+        out.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
+        out.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
+        out.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
+        acc = out;
+      }
+      y[i] = acc;
+      st_release_u32(flag + i, want);  // orders the store of y[i] before the flag
+      done = true;
+    } else if ((++spins & 63) == 0) {
+      if (spins > kSweepSpinLimit) {
+        atomicExch(&sync->err, 1);
+        done = true;
+      } else if (*reinterpret_cast<volatile int*>(&sync->err)) {
+        done = true;
+      }
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence();
+    const unsigned int f = atomicAdd(&sync->done, 1u);
+    if (f == nchunks - 1) {  // every chunk has been claimed and finished
+      sync->claim = 0;
+      sync->done = 0;
+      __threadfence();
+      atomicAdd(&sync->epoch, 1u);
+    }
+  }
 }
 
 }  // namespace o2f

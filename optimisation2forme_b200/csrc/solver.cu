@@ -47,6 +47,7 @@ void validate_params(const o2f_params& p) {
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
   if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
+  if (!(p.adjoint_shift >= 0.0) || !(p.adjoint_shift < 1e6)) throw Error(O2F_ERR_ARG, "adjoint_shift out of range");
 }
 
 }  // namespace
@@ -325,7 +326,7 @@ void Solver::upload_mesh() {
 
 // Reverse Cuthill-McKee order of the cell adjacency graph (BFS from a
 // pseudo-peripheral cell, neighbours by increasing degree, reversed), and the
-// level sets of the forward / backward triangular solves in that order.
+// level sets of the factorization in that order.
 void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector<int2>& ec,
                             const std::vector<uint8_t>& ebc) {
   const int64_t nc = topo_.nc;
@@ -415,21 +416,9 @@ void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector
     nlo = std::max(nlo, l + 1);
   }
   bucket(nlo, lo_off_h_, lo_cells_h_);
-  int nup = 0;
-  for (int64_t i = nc - 1; i >= 0; --i) {
-    const int32_t c = order[i];
-    int l = 0;
-    for (int k = 0; k < 4; ++k) {
-      const int32_t o = nbr(c, k);
-      if (o >= 0 && ilu_pos_h_[o] > i) l = std::max(l, lev[o] + 1);
-    }
-    lev[c] = l;
-    nup = std::max(nup, l + 1);
-  }
-  bucket(nup, up_off_h_, up_cells_h_);
+  ilu_order_h_ = std::move(order);
   ilu_.nc = nc;
   ilu_.n_lo = nlo;
-  ilu_.n_up = nup;
 }
 
 void Solver::ilu_factor() {
@@ -440,24 +429,25 @@ void Solver::ilu_factor() {
     ilu_.pos = arena_.alloc<int32_t>(nc);
     ilu_.A = arena_.alloc<double>(80 * nc);
     ilu_.Dinv = arena_.alloc<double>(16 * nc);
-    ilu_.lo_off = arena_.alloc<int32_t>(lo_off_h_.size());
+    ilu_.order = arena_.alloc<int32_t>(nc);
     ilu_.lo_cells = arena_.alloc<int32_t>(nc);
-    ilu_.up_off = arena_.alloc<int32_t>(up_off_h_.size());
-    ilu_.up_cells = arena_.alloc<int32_t>(nc);
+    ilu_.flag = arena_.alloc<uint32_t>(2 * nc);
+    ilu_.sync = arena_.alloc<SweepSync>(2);
     ilu_status_ = arena_.alloc<int>(1);
     phat_ = arena_.alloc<Vec4<double>>(nc);
     shat_ = arena_.alloc<Vec4<double>>(nc);
     h2d(ilu_.nbr, ilu_nbr_h_, s);
     h2d(ilu_.pos, ilu_pos_h_, s);
-    h2d(ilu_.lo_off, lo_off_h_, s);
+    h2d(ilu_.order, ilu_order_h_, s);
     h2d(ilu_.lo_cells, lo_cells_h_, s);
-    h2d(ilu_.up_off, up_off_h_, s);
-    h2d(ilu_.up_cells, up_cells_h_, s);
+    O2F_CUDA(cudaMemsetAsync(ilu_.flag, 0, 2 * nc * sizeof(uint32_t), s));
+    O2F_CUDA(cudaMemsetAsync(ilu_.sync, 0, 2 * sizeof(SweepSync), s));
     sync();
     ilu_alloc_ = true;
   }
   O2F_CUDA(cudaMemsetAsync(ilu_status_, 0, sizeof(int), s));
-  k_ilu_assemble<<<grid(nc), kBlock, 0, s>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ilu_);
+  k_ilu_assemble<<<grid(nc), kBlock, 0, s>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_,
+                                             params_.adjoint_shift, ilu_);
   for (int l = 0; l < ilu_.n_lo; ++l) {
     const int n = lo_off_h_[l + 1] - lo_off_h_[l];
     k_ilu_factor<<<(n + 127) / 128, 128, 0, s>>>(ilu_.lo_cells + lo_off_h_[l], n, ilu_, ilu_status_);
@@ -471,15 +461,30 @@ void Solver::ilu_factor() {
 }
 
 // z = M^{-1} r: forward levels into z, backward levels in place.
+// z = U^{-1} L^{-1} r: one sync-free launch per triangle, one warp per
+// 32-row chunk (surplus warps of the last block exit without claiming).
 void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) {
   cudaStream_t s = stream_;
-  for (int l = 0; l < ilu_.n_lo; ++l) {
-    const int n = lo_off_h_[l + 1] - lo_off_h_[l];
-    k_ilu_lower<<<(n + 127) / 128, 128, 0, s>>>(ilu_.lo_cells + lo_off_h_[l], n, ilu_, r, z, gate);
-  }
-  for (int l = 0; l < ilu_.n_up; ++l) {
-    const int n = up_off_h_[l + 1] - up_off_h_[l];
-    k_ilu_upper<<<(n + 127) / 128, 128, 0, s>>>(ilu_.up_cells + up_off_h_[l], n, ilu_, z, z, gate);
+  const int n = (int)ilu_.nc;
+  const int chunks = (n + 31) / 32;
+  const int warps_per_block = kSweepBlock / 32;
+  const int blocks = (chunks + warps_per_block - 1) / warps_per_block;
+  k_ilu_sweep<true><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, r, z, gate);
+  k_ilu_sweep<false><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, z, z, gate);
+}
+
+// A sweep whose dependency wait ran out leaves an invalid result: report it
+// (and clear the flag so the context stays usable).
+void Solver::ilu_check_sweeps() {
+  SweepSync h[2];
+  O2F_CUDA(cudaMemcpyAsync(h, ilu_.sync, sizeof(h), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  if (h[0].err || h[1].err) {
+    const int zero[2] = {0, 0};
+    O2F_CUDA(cudaMemcpyAsync(&ilu_.sync[0].err, &zero[0], sizeof(int), cudaMemcpyHostToDevice, stream_));
+    O2F_CUDA(cudaMemcpyAsync(&ilu_.sync[1].err, &zero[1], sizeof(int), cudaMemcpyHostToDevice, stream_));
+    sync();
+    throw Error(O2F_ERR_CUDA, "ILU triangular sweep: dependency wait exceeded its limit");
   }
 }
 
@@ -875,7 +880,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     sh = shat_;
   }
   const int kItersPerGraph = precond ? 1 : 8;
-  const int kernels_per_iter = 5 + (precond ? 2 * (ilu_.n_lo + ilu_.n_up) : 0);
+  const int kernels_per_iter = 5 + (precond ? 4 : 0);
   const int* kgate = &ks_->stop;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
@@ -937,6 +942,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
                                                        reinterpret_cast<double*>(v_), part_, ks_);
         O2F_CUDA(cudaMemcpyAsync(hks, ks_, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream_));
         sync();
+        if (precond) ilu_check_sweeps();
         relres = std::sqrt(hks->rr) / (bnorm > 0 ? bnorm : 1.0);
         if (params_.verbosity >= 1) std::fprintf(stderr, "[adjoint] iters=%lld  relres=%g\n", (long long)total, relres);
         if (relres <= tol) break;

@@ -121,7 +121,8 @@ class Solver {
                       const std::vector<uint8_t>& ebc);
   void ilu_factor();
   void ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate);
-  std::vector<int32_t> ilu_nbr_h_, ilu_pos_h_, lo_off_h_, lo_cells_h_, up_off_h_, up_cells_h_;
+  void ilu_check_sweeps();
+  std::vector<int32_t> ilu_nbr_h_, ilu_pos_h_, ilu_order_h_, lo_off_h_, lo_cells_h_;
   IluDev ilu_{};
   bool ilu_alloc_ = false;
   int* ilu_status_ = nullptr;

@@ -57,6 +57,7 @@ class SimulationParams:
     precision: str = "fp64"
     adjoint_precond: str = "ilu0"
     dt_mode: str = "reference"
+    adjoint_shift: float = 0.0
     max_steps: int = 2**62
     residual_drop: float = 0.0
     adjoint_tol: float = 1e-6
@@ -67,7 +68,7 @@ class SimulationParams:
         p = _lib.Params()
         lib().o2f_params_default(C.byref(p))
         for f in ("gamma", "viscosity", "Pr", "cp", "cfl_number", "final_time", "inflow_velocity", "rho_ref",
-                  "p_ref", "aoa_deg", "limiter_k"):
+                  "p_ref", "aoa_deg", "limiter_k", "adjoint_shift"):
             setattr(p, f, float(getattr(self, f)))
         lim = self.limiter.lower()
         if lim in ("venkatakrishnan", "venkat"):
@@ -84,7 +85,7 @@ class SimulationParams:
 
 
 _FLOAT_KEYS = {"cfl_number", "final_time", "gamma", "viscosity", "Pr", "cp", "inflow_velocity", "rho_ref", "p_ref",
-               "aoa_deg", "limiter_k", "residual_drop", "adjoint_tol"}
+               "aoa_deg", "limiter_k", "residual_drop", "adjoint_tol", "adjoint_shift"}
 _INT_KEYS = {"verbosity", "max_steps", "adjoint_restart", "adjoint_max_iter"}
 _STR_KEYS = {"mesh_name", "boundary_conditions", "initial_condition", "state_load_path", "state_save_path",
              "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond", "dt_mode"}

@@ -46,6 +46,19 @@ ADJOINT_CAP = {"large": 500, "mixed": 500, "small": 100000}
 ADJOINT_ITERS = {"large": 500, "mixed": 500, "small": 350}
 
 
+# DRAM bytes per launch of the dominant kernel from one ncu capture
+# (k_cell_gradient on the 502,656-cell mesh: 131.1 MB read + written),
+# scaled by cells to each workload; None where no capture applies.
+TRAFFIC_PER_CELL = {"cell_gradient": 131.1e6 / 502656}
+
+
+def naca_name(spec) -> str:
+    """Four-digit NACA designation (p digit 0 for a symmetric section)."""
+    m = int(round(spec.m * 100))
+    p = int(round(spec.p * 10)) if m else 0
+    return f"{m}{p}{int(round(spec.t * 100)):02d}"
+
+
 def load_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -236,10 +249,13 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
     dom = max(share, key=share.get)
     peaks = load_peaks()
     achieved = kb[dom] / (prof[dom] / 1e3) / 1e9
+    traffic = args.traffic
+    if traffic is None and dom in TRAFFIC_PER_CELL:
+        traffic = round(TRAFFIC_PER_CELL[dom] * s.n_cells)
     res_ms = sum(prof[k] for k in RESIDUAL_KERNELS)
     res_gbs = residual_bytes(s.n_cells, s.n_edges, s.n_vertices, nnz) / (res_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": args.traffic,
+                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                 "peak_source": peaks["source"], "bytes_per_launch": kb[dom], "launch_ms": round(prof[dom], 5),
                 "residual": {"ms": round(res_ms, 4), "algorithmic_GBs": round(res_gbs, 1),
                              "frac": round(res_gbs / peaks["hbm_gbs"], 4)},
@@ -248,8 +264,8 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded NACA O-grid, freestream start)",
-        "config": {"workload": f"{args.workload}: NACA {int(spec.m * 100)}{int(spec.p * 10)}"
-                               f"{int(round(spec.t * 100)):02d} O-grid, {s.n_cells} triangles, M={flow['mach']:.3f}, "
+        "config": {"workload": f"{args.workload}: NACA {naca_name(spec)} O-grid, {s.n_cells} triangles, "
+                               f"M={flow['mach']:.3f}, "
                                f"AoA={flow['aoa']:.2f}, {rk_steps} SSP-RK3 steps, adjoint tol {args.adjoint_tol}, "
                                "dJ/d(m,p,t)",
                    "cells": s.n_cells, "edges": s.n_edges, "rk_steps": rk_steps, "cfl": params.cfl_number,

@@ -283,6 +283,16 @@ int o2f_get_timing(const o2f_ctx* ctx, o2f_timing* t);
  * ms_out[O2F_K_COUNT]. */
 int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out);
 
+/* No counterpart in the reference.  Residual of the current state (as
+ * o2f_residual, interface states left in the context) and its
+ * ||R_rho||_2 written to *norm_out, with NO device allocation on the call:
+ * the norm reduction's scratch is a static device array of 33,280 bytes.
+ * Limit: meshes of at most 16,777,216 cells (O2F_ERR_ARG beyond).  Calls
+ * that overlap on one device share that scratch and race: serialise them.
+ * The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+int o2f_residual_norm_noalloc(o2f_ctx* ctx, double* norm_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -133,6 +133,7 @@ SIGNATURES = {
     "o2f_cell_permutation": ([_vp, _ip], C.c_int),
     "o2f_get_timing": ([_vp, C.POINTER(Timing)], C.c_int),
     "o2f_profile_kernels": ([_vp, C.c_int, _dp], C.c_int),
+    "o2f_residual_norm_noalloc": ([_vp, _dp], C.c_int),
 }
 
 KERNEL_CLASSES = ["vertex_state", "cell_gradient", "vertex_visc", "edge_flux", "cell_residual", "jt_apply",

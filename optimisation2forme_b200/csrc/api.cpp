@@ -318,6 +318,13 @@ int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out) {
   });
 }
 
+int o2f_residual_norm_noalloc(o2f_ctx* ctx, double* norm_out) {
+  return guarded([&] {
+    need(norm_out, "norm_out");
+    S(ctx).residual_norm_noalloc(norm_out);
+  });
+}
+
 int o2f_get_timing(const o2f_ctx* ctx, o2f_timing* t) {
   return guarded([&] {
     need(t, "timing");

@@ -69,6 +69,7 @@ class Solver {
                       const double* lambda_ref, double* grad);
   void debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which, double* out);
   void profile_kernels(int reps, double* ms_out);
+  void residual_norm_noalloc(double* norm_out);  // noalloc.cu
   double last_residual_ms() const { return last_residual_ms_; }
   int64_t launches() const { return launches_; }
 

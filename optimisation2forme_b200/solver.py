@@ -428,6 +428,13 @@ class Solver:
         check(lib().o2f_profile_kernels(self._h, int(reps), _ptr(ms)))
         return dict(zip(_lib.KERNEL_CLASSES, ms.tolist()))
 
+    def residual_norm_noalloc(self) -> float:
+        """||R_rho||_2 of the current state through o2f_residual_norm_noalloc
+        (no device allocation on the call; one call at a time per device)."""
+        out = C.c_double()
+        check(lib().o2f_residual_norm_noalloc(self._h, C.byref(out)))
+        return out.value
+
     def timing(self) -> dict:
         t = _lib.Timing()
         check(lib().o2f_get_timing(self._h, C.byref(t)))

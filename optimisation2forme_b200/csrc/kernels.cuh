@@ -264,9 +264,26 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
   const Vec4<T> cg = g.cgeom[c];
   const T cx = cg.a, cy = cg.b, cv = cg.c, veps = cg.d;
   const Vec4<T> u = U[c];
-  int sl[4];
+  // The cell's edges are the slots before the first empty one.  All index
+  // and geometry loads of every edge are issued before the arithmetic, so
+  // the gathers of one cell overlap instead of forming one chain per edge.
+  int sl[4], nk = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) sl[k] = slot[(int64_t)k * nc + c];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (sl[k] >= 0 && nk == k) nk = k + 1;
+  int2 evv[4], cc[4];
+  uint8_t code[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k < nk) {
+      const int e = sl[k] >> 1;
+      evv[k] = ev[e];
+      cc[k] = ec[e];
+      code[k] = ebc[e];
+    }
+  }
 
   T gx0 = (T)0.0, gx1 = (T)0.0, gx2 = (T)0.0, gx3 = (T)0.0;
   T gy0 = (T)0.0, gy1 = (T)0.0, gy2 = (T)0.0, gy3 = (T)0.0;
@@ -274,19 +291,20 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
   T mx0 = u.a, mx1 = u.b, mx2 = u.c, mx3 = u.d;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
+    if (k >= nk) continue;
     const int s = sl[k];
-    if (s < 0) break;
     const int e = s >> 1;
     const bool left = (s & 1) == 0;
-    const int2 vv = ev[e];
-    const Vec4<T> va = vq[vv.x], vb = vq[vv.y];
+    const Vec4<T> va = vq[evv[k].x], vb = vq[evv[k].y];
+    const Vec4<T> eg = g.egeom[e];
+    const int o = left ? cc[k].y : cc[k].x;
+    Vec4<T> un = u;
+    if (o >= 0) un = U[o];
     T er = (T)0.5 * (va.a + vb.a);
     T eru = (T)0.5 * (va.b + vb.b);
     T erv = (T)0.5 * (va.c + vb.c);
     T eE = (T)0.5 * (va.d + vb.d);
-    const uint8_t code = ebc[e];
-    if (code) bc_state(code, ph, er, eru, erv, eE);
-    const Vec4<T> eg = g.egeom[e];
+    if (code[k]) bc_state(code[k], ph, er, eru, erv, eE);
     const T el = eg.c;
     T enx = eg.a, eny = eg.b;
     if (left) {
@@ -301,10 +319,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
     gy1 += eru * el * eny / cv;
     gy2 += erv * el * eny / cv;
     gy3 += eE * el * eny / cv;
-    const int2 cc = ec[e];
-    const int o = left ? cc.y : cc.x;
     if (o >= 0) {
-      const Vec4<T> un = U[o];
       if (un.a < mn0) mn0 = un.a;
       if (un.a > mx0) mx0 = un.a;
       if (un.b < mn1) mn1 = un.b;
@@ -318,12 +333,14 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
 
   const int kind = ph.limiter;
   T al0 = (T)1.0, al1 = (T)1.0, al2 = (T)1.0, al3 = (T)1.0;
+  T dxk[4], dyk[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const int s = sl[k];
-    if (s < 0) break;
-    const Vec2<T> ce = g.ectr[s >> 1];
+    if (k >= nk) continue;
+    const Vec2<T> ce = g.ectr[sl[k] >> 1];
     const T dx = ce.a - cx, dy = ce.b - cy;
+    dxk[k] = dx;
+    dyk[k] = dy;
     al0 = smin(al0, limiter_alpha(kind, u.a, u.a + gx0 * dx + gy0 * dy, mn0, mx0, veps));
     al1 = smin(al1, limiter_alpha(kind, u.b, u.b + gx1 * dx + gy1 * dy, mn1, mx1, veps));
     al2 = smin(al2, limiter_alpha(kind, u.c, u.c + gx2 * dx + gy2 * dy, mn2, mx2, veps));
@@ -331,17 +348,15 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
+    if (k >= nk) continue;
     const int s = sl[k];
-    if (s < 0) break;
     const int e = s >> 1;
-    const Vec2<T> ce = g.ectr[e];
-    const T dx = ce.a - cx, dy = ce.b - cy;
+    const T dx = dxk[k], dy = dyk[k];
     const Vec4<T> st = v4<T>(u.a + al0 * (gx0 * dx + gy0 * dy), u.b + al1 * (gx1 * dx + gy1 * dy),
                              u.c + al2 * (gx2 * dx + gy2 * dy), u.d + al3 * (gx3 * dx + gy3 * dy));
     if ((s & 1) == 0) {
       eL[e] = st;
-      const uint8_t code = ebc[e];
-      if (code) eR[e] = bc_ghost(code, ph, st);
+      if (code[k]) eR[e] = bc_ghost(code[k], ph, st);
     } else {
       eR[e] = st;
     }

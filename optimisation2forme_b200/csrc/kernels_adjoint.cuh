@@ -277,10 +277,31 @@ __global__ void __launch_bounds__(128) k_jt_blocks(int64_t ne, Geom<double> g, c
 //   y_c  += F_{U_side}^T Delta.
 // Deterministic: no atomics.  Optional fused epilogue: dots of y with up to
 // two other vectors, reduced over the grid (kDots), for BiCGSTAB.
-template <int kDots>
+// One 4x4 Jacobian block into registers: FP64 blocks as stored, FP32 blocks
+// (the mixed-precision path) widened to FP64 for the accumulation.
+__device__ __forceinline__ void load_block(const double* B, double* b) {
+#pragma unroll
+  for (int i = 0; i < 16; i += 2) {
+    const double2 t = *reinterpret_cast<const double2*>(B + i);
+    b[i] = t.x;
+    b[i + 1] = t.y;
+  }
+}
+__device__ __forceinline__ void load_block(const float* B, double* b) {
+#pragma unroll
+  for (int i = 0; i < 16; i += 4) {
+    const float4 t = *reinterpret_cast<const float4*>(B + i);
+    b[i] = (double)t.x;
+    b[i + 1] = (double)t.y;
+    b[i + 2] = (double)t.z;
+    b[i + 3] = (double)t.w;
+  }
+}
+
+template <int kDots, typename TB>
 __device__ __forceinline__ void jt_cell(int64_t c, int64_t nc, const int32_t* __restrict__ jslot, Geom<double> g,
                                         const int2* __restrict__ ec, const uint8_t* __restrict__ ebc,
-                                        const double* __restrict__ blk, const Vec4<double>* __restrict__ x,
+                                        const TB* __restrict__ blk, const Vec4<double>* __restrict__ x,
                                         Vec4<double>& y) {
   const Vec4<double> xc = x[c];
   const double invVc = 1.0 / g.cgeom[c].c;
@@ -293,7 +314,7 @@ __device__ __forceinline__ void jt_cell(int64_t c, int64_t nc, const int32_t* __
     const bool left = (s & 1) == 0;
     const double L = g.egeom[e].c;
     double d0, d1, d2, d3;
-    const double* B;
+    const TB* B;
     if (ebc[e] != 0) {
       d0 = (-xc.a * invVc) * L;
       d1 = (-xc.b * invVc) * L;
@@ -313,12 +334,7 @@ __device__ __forceinline__ void jt_cell(int64_t c, int64_t nc, const int32_t* __
       B = blk + (int64_t)e * 32 + (left ? 0 : 16);
     }
     double b[16];
-#pragma unroll
-    for (int i = 0; i < 16; i += 2) {
-      const double2 t = *reinterpret_cast<const double2*>(B + i);
-      b[i] = t.x;
-      b[i + 1] = t.y;
-    }
+    load_block(B, b);
     y.a += (b[0] * d0 + b[4] * d1 + b[8] * d2 + b[12] * d3);
     y.b += (b[1] * d0 + b[5] * d1 + b[9] * d2 + b[13] * d3);
     y.c += (b[2] * d0 + b[6] * d1 + b[10] * d2 + b[14] * d3);
@@ -326,14 +342,15 @@ __device__ __forceinline__ void jt_cell(int64_t c, int64_t nc, const int32_t* __
   }
 }
 
+template <typename TB>
 __global__ void __launch_bounds__(kBlock) k_jt_apply(int64_t nc, const int32_t* __restrict__ jslot, Geom<double> g,
                                                      const int2* __restrict__ ec, const uint8_t* __restrict__ ebc,
-                                                     const double* __restrict__ blk,
+                                                     const TB* __restrict__ blk,
                                                      const Vec4<double>* __restrict__ x, Vec4<double>* __restrict__ y) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   Vec4<double> r;
-  jt_cell<0>(c, nc, jslot, g, ec, ebc, blk, x, r);
+  jt_cell<0, TB>(c, nc, jslot, g, ec, ebc, blk, x, r);
   y[c] = r;
 }
 
@@ -442,9 +459,10 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(int64_t n4, const double* __r
 }
 
 // v = J^T p with the fused dot (r0, v); epilogue alpha = rho / (r0, v).
+template <typename TB>
 __global__ void __launch_bounds__(kBlock) k_bicg_jt_v(int64_t nc, const int32_t* __restrict__ jslot, Geom<double> g,
                                                       const int2* __restrict__ ec, const uint8_t* __restrict__ ebc,
-                                                      const double* __restrict__ blk,
+                                                      const TB* __restrict__ blk,
                                                       const Vec4<double>* __restrict__ p, Vec4<double>* __restrict__ v,
                                                       const Vec4<double>* __restrict__ r0, double* part,
                                                       KrylovState* ks) {
@@ -452,7 +470,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_jt_v(int64_t nc, const int32_t*
   double acc[1] = {0.0};
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
     Vec4<double> y;
-    jt_cell<0>(c, nc, jslot, g, ec, ebc, blk, p, y);
+    jt_cell<0, TB>(c, nc, jslot, g, ec, ebc, blk, p, y);
     v[c] = y;
     const Vec4<double> q = r0[c];
     acc[0] += q.a * y.a + q.b * y.b + q.c * y.c + q.d * y.d;
@@ -477,9 +495,10 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(int64_t n4, const double* __r
 
 // t = J^T shat (shat = M^{-1} s, or s itself without preconditioner) with the
 // fused dots (t, t), (t, s); epilogue omega.
+template <typename TB>
 __global__ void __launch_bounds__(kBlock) k_bicg_jt_t(int64_t nc, const int32_t* __restrict__ jslot, Geom<double> g,
                                                       const int2* __restrict__ ec, const uint8_t* __restrict__ ebc,
-                                                      const double* __restrict__ blk,
+                                                      const TB* __restrict__ blk,
                                                       const Vec4<double>* __restrict__ shat,
                                                       const Vec4<double>* __restrict__ s, Vec4<double>* __restrict__ t,
                                                       double* part, KrylovState* ks) {
@@ -487,7 +506,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_jt_t(int64_t nc, const int32_t*
   double acc[2] = {0.0, 0.0};
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
     Vec4<double> y;
-    jt_cell<0>(c, nc, jslot, g, ec, ebc, blk, shat, y);
+    jt_cell<0, TB>(c, nc, jslot, g, ec, ebc, blk, shat, y);
     t[c] = y;
     const Vec4<double> q = s[c];
     acc[0] += y.a * y.a + y.b * y.b + y.c * y.c + y.d * y.d;

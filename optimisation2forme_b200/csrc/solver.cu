@@ -43,7 +43,7 @@ void validate_params(const o2f_params& p) {
     throw Error(O2F_ERR_ARG, "invalid physical parameters");
   if (p.limiter != O2F_LIMITER_VENKAT && p.limiter != O2F_LIMITER_BARTH_JESPERSEN)
     throw Error(O2F_ERR_ARG, "unknown limiter");
-  if (p.precision != O2F_PREC_F64) throw Error(O2F_ERR_ARG, "this context supports O2F_PREC_F64");
+  if (p.precision != O2F_PREC_F64 && p.precision != O2F_PREC_F32) throw Error(O2F_ERR_ARG, "unknown precision");
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
   if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
@@ -131,6 +131,7 @@ void Solver::set_params(const o2f_params& p) {
   k_venkat_eps<double><<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, p.limiter_k, geom_.cgeom);
   O2F_CUDA(cudaGetLastError());
   blk_valid_ = false;
+  f32_geom_valid_ = false;  // the FP32 geometry copy holds the old limiter eps
 }
 
 void Solver::upload_mesh() {
@@ -596,9 +597,17 @@ void Solver::launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<
 }
 
 void Solver::residual(double* R_ref) {
+  if (f32()) {
+    ensure_f32();
+    f32_state_sync();
+  }
   O2F_CUDA(cudaEventRecord(ev0_, stream_));
-  launch_residual(geom_, work_, U_, nullptr, true, nullptr);
+  if (f32())
+    launch_residual_f32(nullptr, nullptr);
+  else
+    launch_residual(geom_, work_, U_, nullptr, true, nullptr);
   O2F_CUDA(cudaEventRecord(ev1_, stream_));
+  if (f32()) f32_publish_interfaces();
   sync();
   float ms = 0.f;
   O2F_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
@@ -745,6 +754,19 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
   // One CUDA graph holds kStepsPerGraph steps; steps past a stop condition
   // are no-ops (every kernel checks the gate).
   const int kStepsPerGraph = topo_.nc < 200000 ? 16 : 4;
+  // FP64 path: the reference arithmetic.  Mixed path: FP32 residual, FP64
+  // state update (solver_f32.cu).
+  const bool mixed = f32();
+  if (mixed) {
+    ensure_f32();
+    f32_state_sync();
+  }
+  auto stage = [&](const RkStage* rk) {
+    if (mixed)
+      launch_residual_f32(gate, rk);
+    else
+      launch_residual(geom_, work_, U_, gate, false, rk);
+  };
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   O2F_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -752,10 +774,10 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
     k_step_begin<<<1, 1, 0, stream_>>>(step_);
     k_wave_speed<double><<<wave_grid, kBlock, 0, stream_>>>(topo_.nc, U_, params_.gamma, step_);
     k_step_dt<<<1, 1, 0, stream_>>>(step_);
-    launch_residual(geom_, work_, U_, gate, false, &s1);
+    stage(&s1);
     k_step_norm<<<1, 1024, 0, stream_>>>(norm_part_, nparts, hist_dev_, step_);
-    launch_residual(geom_, work_, U_, gate, false, &s2);
-    launch_residual(geom_, work_, U_, gate, false, &s3);
+    stage(&s2);
+    stage(&s3);
     k_step_end<<<1, 1, 0, stream_>>>(step_);
   }
   O2F_CUDA(cudaStreamEndCapture(stream_, &graph));
@@ -789,6 +811,7 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
                         cudaMemcpyDeviceToHost));
   if (steps_done) *steps_done = fin.step;
   if (t_out) *t_out = fin.t;
+  if (mixed && fin.step > 0) f32_publish_interfaces();
   have_residual_ = fin.step > 0;
   blk_valid_ = false;
   if (fin.stop == 2) throw Error(O2F_ERR_NONFINITE, "non-finite state or residual in the time loop");
@@ -810,6 +833,7 @@ void Solver::build_jt_blocks() {
   k_jt_blocks<<<(int)((topo_.ne + 127) / 128), 128, 0, stream_>>>(topo_.ne, geom_, topo_.ebc, work_.eL, work_.eR,
                                                                    phys_, 1e-6, blk_);
   O2F_CUDA(cudaGetLastError());
+  if (f32()) f32_blocks();
   blk_valid_ = true;
 }
 
@@ -823,7 +847,13 @@ void Solver::jt_apply(const double* x_ref, double* y_ref) {
   if (!tmp_) tmp_ = arena_.alloc<Vec4<double>>(topo_.nc);
   if (!s_) s_ = arena_.alloc<Vec4<double>>(topo_.nc);
   to_internal(x_ref, s_);
-  jt_apply_dev(s_, tmp_);
+  if (f32()) {
+    k_jt_apply<<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, s_,
+                                                       tmp_);
+    O2F_CUDA(cudaGetLastError());
+  } else {
+    jt_apply_dev(s_, tmp_);
+  }
   to_reference(tmp_, y_ref);
 }
 
@@ -889,13 +919,21 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     k_bicg_p<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_),
                                                reinterpret_cast<double*>(p_), reinterpret_cast<double*>(v_), ks_);
     if (precond) ilu_apply(p_, ph, kgate);
-    k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ph, v_, r0_,
-                                                  part_, ks_);
+    if (f32())  // FP32 blocks; restarts take the true residual with the FP64 operator
+      k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, ph, v_, r0_,
+                                                    part_, ks_);
+    else
+      k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ph, v_, r0_,
+                                                    part_, ks_);
     k_bicg_s<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(v_),
                                                reinterpret_cast<double*>(s_), ks_);
     if (precond) ilu_apply(s_, sh, kgate);
-    k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, sh, s_, t_,
-                                                  part_, ks_);
+    if (f32())
+      k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, sh, s_, t_,
+                                                    part_, ks_);
+    else
+      k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, sh, s_, t_,
+                                                    part_, ks_);
     k_bicg_xr<<<kRedGrid, kBlock, 0, stream_>>>(n4, x, reinterpret_cast<double*>(ph), reinterpret_cast<double*>(sh),
                                                 reinterpret_cast<double*>(s_), reinterpret_cast<double*>(t_),
                                                 reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_), part_,

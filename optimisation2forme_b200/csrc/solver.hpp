@@ -83,6 +83,14 @@ class Solver {
   void perturbed_geometry(const o2f_shape_params& sp, int id, double eps);
   void ensure_pert_buffers();
   Work<double> alloc_work();
+  // mixed precision (solver_f32.cu)
+  bool f32() const { return params_.precision == O2F_PREC_F32; }
+  Work<float> alloc_work_f32();
+  void ensure_f32();
+  void f32_state_sync();
+  void f32_publish_interfaces();
+  void launch_residual_f32(const int* gate, const void* rk);
+  void f32_blocks();
   void to_internal(const double* ref, Vec4<double>* dev);
   void to_reference(const Vec4<double>* dev, double* ref);
   void sync();
@@ -102,6 +110,12 @@ class Solver {
   Work<double> work_{};
   Vec4<double>* U_ = nullptr;
   Vec4<double>* Uold_ = nullptr;
+  bool f32_ready_ = false;
+  bool f32_geom_valid_ = false;
+  Geom<float> geom32_{};
+  Work<float> work32_{};
+  Vec4<float>* U32_ = nullptr;
+  float* blk32_ = nullptr;
   double* norm_part_ = nullptr;
   StepState* step_ = nullptr;
   double* hist_dev_ = nullptr;

@@ -283,6 +283,34 @@ int o2f_get_timing(const o2f_ctx* ctx, o2f_timing* t);
  * ms_out[O2F_K_COUNT]. */
 int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out);
 
+/* Batched time loop (no reference counterpart: the reference solves one
+ * candidate per process, run_opti.sh).  A batch references n existing
+ * FP64 contexts (each with its own mesh, flow parameters and state; all on
+ * one device, the batch runs on the first context's stream); the contexts
+ * must outlive the batch and must not be used while a batch call runs.
+ * o2f_batch_rk3_run advances every candidate by SSP-RK3 exactly as
+ * o2f_rk3_run would (bit-identical FP64 states, each candidate with its own
+ * dt and stop condition) with one grouped launch per phase for the whole
+ * batch, captured in a CUDA graph.  Per candidate: steps_done, t_out,
+ * status_out (O2F_OK or O2F_ERR_NONFINITE); any may be NULL.  After the run
+ * each context holds the interface states of its last stage, so
+ * o2f_forces / o2f_adjoint_solve / o2f_shape_gradient apply per context. */
+typedef struct o2f_batch o2f_batch;
+int o2f_batch_create(o2f_ctx* const* ctxs, int n, o2f_batch** out);
+int o2f_batch_destroy(o2f_batch* batch);
+/* Autotuner: times every phase of the grouped step with block sizes
+ * 128/256/512 and 1/2/4 entities per thread (reps launches each, CUDA
+ * events), keeps the fastest, and caches it for batches of the same size
+ * bucket (log2 of the total cells).  config_out (may be NULL) receives
+ * {block, tile} for the O2F_BATCH_PHASES phases: vertex state, cell
+ * gradient, vertex viscous, edge flux, cell residual, wave speed. */
+#define O2F_BATCH_PHASES 6
+int o2f_batch_tune(o2f_batch* batch, int reps, int* config_out);
+int o2f_batch_rk3_run(o2f_batch* batch, int64_t max_steps, double drop_tol, int64_t* steps_done, double* t_out,
+                      int* status_out);
+/* ||R_rho||_2 history of candidate `index` from the last o2f_batch_rk3_run. */
+int o2f_batch_history(o2f_batch* batch, int index, double* history_host, int64_t count);
+
 /* No counterpart in the reference.  Residual of the current state (as
  * o2f_residual, interface states left in the context) and its
  * ||R_rho||_2 written to *norm_out, with NO device allocation on the call:

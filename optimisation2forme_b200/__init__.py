@@ -6,8 +6,8 @@ The compute lives in the native library ``libo2f.so`` (C ABI in
 binding.  Importing works without a GPU; creating a ``Solver`` needs one.
 """
 from ._lib import LIB_PATH, O2FError, lib
-from .solver import (HostMesh, SimulationParams, Solver, load_cell_states, load_config, load_params_generic,
+from .solver import (Batch, HostMesh, SimulationParams, Solver, load_cell_states, load_config, load_params_generic,
                      mesh_desc, save_cell_states, write_shape_log)
 
-__all__ = ["LIB_PATH", "O2FError", "lib", "HostMesh", "SimulationParams", "Solver", "load_cell_states",
+__all__ = ["LIB_PATH", "O2FError", "lib", "Batch", "HostMesh", "SimulationParams", "Solver", "load_cell_states",
            "load_config", "load_params_generic", "mesh_desc", "save_cell_states", "write_shape_log"]

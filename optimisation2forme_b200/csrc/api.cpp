@@ -7,7 +7,9 @@
 #include <ios>
 #include <memory>
 #include <string>
+#include <vector>
 
+#include "batch.hpp"
 #include "mesh_host.hpp"
 #include "o2f.h"
 #include "solver.hpp"
@@ -18,6 +20,10 @@ struct o2f_ctx {
 
 struct o2f_host_mesh {
   o2f::HostMesh mesh;
+};
+
+struct o2f_batch {
+  std::unique_ptr<o2f::Batch> batch;
 };
 
 namespace {
@@ -315,6 +321,47 @@ int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out) {
   return guarded([&] {
     need(ms_out, "ms_out");
     S(ctx).profile_kernels(reps, ms_out);
+  });
+}
+
+int o2f_batch_create(o2f_ctx* const* ctxs, int n, o2f_batch** out) {
+  return guarded([&] {
+    need(ctxs, "ctxs");
+    need(out, "out");
+    *out = nullptr;
+    if (n <= 0) throw o2f::Error(O2F_ERR_ARG, "a batch needs at least one context");
+    std::vector<o2f::Solver*> v;
+    for (int i = 0; i < n; ++i) v.push_back(&S(ctxs[i]));
+    auto b = std::make_unique<o2f_batch>();
+    b->batch = std::make_unique<o2f::Batch>(std::move(v));
+    *out = b.release();
+  });
+}
+
+int o2f_batch_destroy(o2f_batch* batch) {
+  return guarded([&] { delete batch; });
+}
+
+namespace {
+o2f::Batch& B(o2f_batch* b) {
+  if (!b || !b->batch) throw o2f::Error(O2F_ERR_ARG, "null batch");
+  return *b->batch;
+}
+}  // namespace
+
+int o2f_batch_tune(o2f_batch* batch, int reps, int* config_out) {
+  return guarded([&] { B(batch).tune(reps, config_out); });
+}
+
+int o2f_batch_rk3_run(o2f_batch* batch, int64_t max_steps, double drop_tol, int64_t* steps_done, double* t_out,
+                      int* status_out) {
+  return guarded([&] { B(batch).rk3_run(max_steps, drop_tol, steps_done, t_out, status_out); });
+}
+
+int o2f_batch_history(o2f_batch* batch, int index, double* history_host, int64_t count) {
+  return guarded([&] {
+    need(history_host, "history");
+    B(batch).history(index, history_host, count);
   });
 }
 

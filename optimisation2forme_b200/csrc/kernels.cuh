@@ -171,15 +171,12 @@ __device__ __forceinline__ T limiter_alpha(int kind, T phi_i, T phi_pred, T phi_
 // of the reference exactly: w=1 copies, w=0.5 halves, and the 3- and 4-cell
 // sums keep the reference's left-to-right association.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_vertex_state(int64_t nv, const int32_t* __restrict__ voff,
+__device__ __forceinline__ void vertex_state_at(int64_t v, int64_t nv, const int32_t* __restrict__ voff,
                                                          const int32_t* __restrict__ vcid,
                                                          const T* __restrict__ vw,
                                                          const uint8_t* __restrict__ vbc,
                                                          const Vec4<T>* __restrict__ U, Phys ph,
-                                                         Vec4<T>* __restrict__ vq, const int* gate) {
-  if (gated(gate)) return;
-  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
+                                                         Vec4<T>* __restrict__ vq) {
   const int o0 = voff[v], o1 = voff[v + 1];
   T a = (T)0.0, b = (T)0.0, c = (T)0.0, d = (T)0.0;
   if (o1 > o0) {
@@ -203,21 +200,30 @@ __global__ void __launch_bounds__(kBlock) k_vertex_state(int64_t nv, const int32
   vq[v] = v4<T>(a, b, c, d);
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_vertex_state(int64_t nv, const int32_t* __restrict__ voff,
+                                                         const int32_t* __restrict__ vcid,
+                                                         const T* __restrict__ vw,
+                                                         const uint8_t* __restrict__ vbc,
+                                                         const Vec4<T>* __restrict__ U, Phys ph,
+                                                         Vec4<T>* __restrict__ vq, const int* gate) {
+  if (gated(gate)) return;
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  vertex_state_at<T>(v, nv, voff, vcid, vw, vbc, U, ph, vq);
+}
+
 // K3: the same interpolation for the five viscous quantities
 // (src/diffusion.cpp:29-140) with apply_diffusion_bc (src/boundary.cpp:101-127):
 // far field and wall vertices are zeroed.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_vertex_visc(int64_t nv, const int32_t* __restrict__ voff,
+__device__ __forceinline__ void vertex_visc_at(int64_t v, int64_t nv, const int32_t* __restrict__ voff,
                                                         const int32_t* __restrict__ vcid,
                                                         const T* __restrict__ vw,
                                                         const uint8_t* __restrict__ vbc,
                                                         const Vec4<T>* __restrict__ ctq,
                                                         const T* __restrict__ ctqy,
-                                                        Vec4<T>* __restrict__ vtq, T* __restrict__ vtqy,
-                                                        const int* gate) {
-  if (gated(gate)) return;
-  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
+                                                        Vec4<T>* __restrict__ vtq, T* __restrict__ vtqy) {
   const int o0 = voff[v], o1 = voff[v + 1];
   T a = (T)0.0, b = (T)0.0, c = (T)0.0, d = (T)0.0, e = (T)0.0;
   if (o1 > o0) {
@@ -248,19 +254,31 @@ __global__ void __launch_bounds__(kBlock) k_vertex_visc(int64_t nv, const int32_
   vtqy[v] = e;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_vertex_visc(int64_t nv, const int32_t* __restrict__ voff,
+                                                        const int32_t* __restrict__ vcid,
+                                                        const T* __restrict__ vw,
+                                                        const uint8_t* __restrict__ vbc,
+                                                        const Vec4<T>* __restrict__ ctq,
+                                                        const T* __restrict__ ctqy,
+                                                        Vec4<T>* __restrict__ vtq, T* __restrict__ vtqy,
+                                                        const int* gate) {
+  if (gated(gate)) return;
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  vertex_visc_at<T>(v, nv, voff, vcid, vw, vbc, ctq, ctqy, vtq, vtqy);
+}
+
 // K2: per cell -- edge values from the vertex states and the Green-Gauss
 // gradient (src/advection.cpp:136-188), neighbour min/max, limiter and
 // interface states (:236-321), and the cell viscous stress and heat flux from
 // the unlimited gradients (src/diffusion.cpp:223-241).
 template <typename T, bool kWriteGrad>
-__global__ void __launch_bounds__(kBlock) k_cell_gradient(
+__device__ __forceinline__ void cell_gradient_at(int64_t c, 
     int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
     const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
     const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
-    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad, const int* gate) {
-  if (gated(gate)) return;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad) {
   const Vec4<T> cg = g.cgeom[c];
   const T cx = cg.a, cy = cg.b, cv = cg.c, veps = cg.d;
   const Vec4<T> u = U[c];
@@ -384,20 +402,29 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
   }
 }
 
+template <typename T, bool kWriteGrad>
+__global__ void __launch_bounds__(kBlock) k_cell_gradient(
+    int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
+    const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
+    const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad, const int* gate) {
+  if (gated(gate)) return;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  cell_gradient_at<T, kWriteGrad>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad);
+}
+
 // K4: per edge -- HLLC flux (src/advection.cpp:433-437) and the edge viscous
 // quantities with their boundary conditions (src/diffusion.cpp:145-170).
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_edge_flux(int64_t ne, Geom<T> g, const int2* __restrict__ ev,
+__device__ __forceinline__ void edge_flux_at(int64_t e, int64_t ne, Geom<T> g, const int2* __restrict__ ev,
                                                       const uint8_t* __restrict__ ebc,
                                                       const Vec4<T>* __restrict__ eL,
                                                       const Vec4<T>* __restrict__ eR,
                                                       const Vec4<T>* __restrict__ vtq,
                                                       const T* __restrict__ vtqy, Phys ph,
                                                       Vec4<T>* __restrict__ F, Vec4<T>* __restrict__ etq,
-                                                      T* __restrict__ etqy, const int* gate) {
-  if (gated(gate)) return;
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= ne) return;
+                                                      T* __restrict__ etqy) {
   const Vec4<T> eg = g.egeom[e];
   F[e] = hllc(eL[e], eR[e], eg.a, eg.b, (T)ph.gamma);
   const int2 vv = ev[e];
@@ -411,6 +438,21 @@ __global__ void __launch_bounds__(kBlock) k_edge_flux(int64_t ne, Geom<T> g, con
   if (code == 'f' || code == 'w') txx = tyy = txy = qx = qy = (T)0.0;
   etq[e] = v4<T>(txx, tyy, txy, qx);
   etqy[e] = qy;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_edge_flux(int64_t ne, Geom<T> g, const int2* __restrict__ ev,
+                                                      const uint8_t* __restrict__ ebc,
+                                                      const Vec4<T>* __restrict__ eL,
+                                                      const Vec4<T>* __restrict__ eR,
+                                                      const Vec4<T>* __restrict__ vtq,
+                                                      const T* __restrict__ vtqy, Phys ph,
+                                                      Vec4<T>* __restrict__ F, Vec4<T>* __restrict__ etq,
+                                                      T* __restrict__ etqy, const int* gate) {
+  if (gated(gate)) return;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  edge_flux_at<T>(e, ne, g, ev, ebc, eL, eR, vtq, vtqy, ph, F, etq, etqy);
 }
 
 // Partial sum of squares of a block, written to part[blockIdx.x].
@@ -438,6 +480,80 @@ struct RkStage {
 // (src/advection.cpp:439-464), then the viscous Green-Gauss divergence added
 // to R (src/diffusion.cpp:176-201).  kRk fuses the SSP-RK3 stage update of
 // Simulator::rk3_substep (src/simulation.cpp:159-167).
+// Returns R_rho^2 of cell c for the residual-norm partial sums (0 unless
+// kRk with norm partials requested).
+template <typename T, bool kRk>
+__device__ __forceinline__ double cell_residual_at(int64_t c, int64_t nc, const int32_t* __restrict__ slot, Geom<T> g,
+                                                   const Vec4<T>* __restrict__ F, const Vec4<T>* __restrict__ etq,
+                                                   const T* __restrict__ etqy, Vec4<T>* __restrict__ U,
+                                                   Vec4<T>* __restrict__ Uold, Vec4<T>* __restrict__ R,
+                                                   const RkStage& rk) {
+  double r2 = 0.0;
+  const T cv = g.cgeom[c].c;
+  int sl[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) sl[k] = slot[(int64_t)k * nc + c];
+  T a0 = (T)0.0, a1 = (T)0.0, a2 = (T)0.0, a3 = (T)0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int s = sl[k];
+    if (s < 0) break;
+    const int e = s >> 1;
+    const T sign = ((s & 1) == 0) ? (T)1.0 : (T)-1.0;
+    const T L = g.egeom[e].c;
+    const Vec4<T> f = F[e];
+    a0 += sign * f.a * L;
+    a1 += sign * f.b * L;
+    a2 += sign * f.c * L;
+    a3 += sign * f.d * L;
+  }
+  const T invV = (T)1.0 / cv;
+  a0 *= -invV;
+  a1 *= -invV;
+  a2 *= -invV;
+  a3 *= -invV;
+  Vec4<T> u = U[c];
+  const T uu = u.b / u.a;
+  const T vv = u.c / u.a;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int s = sl[k];
+    if (s < 0) break;
+    const int e = s >> 1;
+    const Vec4<T> eg = g.egeom[e];
+    const T el = eg.c;
+    T enx = eg.a, eny = eg.b;
+    if ((s & 1) == 0) {
+      enx = -enx;
+      eny = -eny;
+    }
+    const Vec4<T> t = etq[e];
+    const T qy = etqy[e];
+    a1 += t.a * el * enx / cv + t.c * el * eny / cv;
+    a2 += t.c * el * enx / cv + t.b * el * eny / cv;
+    a3 += (uu * t.a + vv * t.c - t.d) * el * enx / cv + (uu * t.c + vv * t.b - qy) * el * eny / cv;
+  }
+  R[c] = v4<T>(a0, a1, a2, a3);
+  if (kRk) {
+    if (rk.norm_part) r2 = (double)a0 * (double)a0;
+    const T dt = (T)(*rk.dt);
+    const T c0 = (T)rk.c0, c1 = (T)rk.c1;
+    Vec4<T> uo;
+    if (rk.snapshot) {
+      uo = u;
+      Uold[c] = u;
+    } else {
+      uo = Uold[c];
+    }
+    u.a = c0 * uo.a + c1 * (u.a + dt * (a0));
+    u.b = c0 * uo.b + c1 * (u.b + dt * (a1));
+    u.c = c0 * uo.c + c1 * (u.c + dt * (a2));
+    u.d = c0 * uo.d + c1 * (u.d + dt * (a3));
+    U[c] = u;
+  }
+  return r2;
+}
+
 template <typename T, bool kRk>
 __global__ void __launch_bounds__(kBlock) k_cell_residual(int64_t nc, const int32_t* __restrict__ slot, Geom<T> g,
                                                           const Vec4<T>* __restrict__ F,
@@ -449,70 +565,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_residual(int64_t nc, const int3
   if (gated(gate)) return;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double r2 = 0.0;
-  if (c < nc) {
-    const T cv = g.cgeom[c].c;
-    int sl[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) sl[k] = slot[(int64_t)k * nc + c];
-    T a0 = (T)0.0, a1 = (T)0.0, a2 = (T)0.0, a3 = (T)0.0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int s = sl[k];
-      if (s < 0) break;
-      const int e = s >> 1;
-      const T sign = ((s & 1) == 0) ? (T)1.0 : (T)-1.0;
-      const T L = g.egeom[e].c;
-      const Vec4<T> f = F[e];
-      a0 += sign * f.a * L;
-      a1 += sign * f.b * L;
-      a2 += sign * f.c * L;
-      a3 += sign * f.d * L;
-    }
-    const T invV = (T)1.0 / cv;
-    a0 *= -invV;
-    a1 *= -invV;
-    a2 *= -invV;
-    a3 *= -invV;
-    Vec4<T> u = U[c];
-    const T uu = u.b / u.a;
-    const T vv = u.c / u.a;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int s = sl[k];
-      if (s < 0) break;
-      const int e = s >> 1;
-      const Vec4<T> eg = g.egeom[e];
-      const T el = eg.c;
-      T enx = eg.a, eny = eg.b;
-      if ((s & 1) == 0) {
-        enx = -enx;
-        eny = -eny;
-      }
-      const Vec4<T> t = etq[e];
-      const T qy = etqy[e];
-      a1 += t.a * el * enx / cv + t.c * el * eny / cv;
-      a2 += t.c * el * enx / cv + t.b * el * eny / cv;
-      a3 += (uu * t.a + vv * t.c - t.d) * el * enx / cv + (uu * t.c + vv * t.b - qy) * el * eny / cv;
-    }
-    R[c] = v4<T>(a0, a1, a2, a3);
-    if (kRk) {
-      if (rk.norm_part) r2 = (double)a0 * (double)a0;
-      const T dt = (T)(*rk.dt);
-      const T c0 = (T)rk.c0, c1 = (T)rk.c1;
-      Vec4<T> uo;
-      if (rk.snapshot) {
-        uo = u;
-        Uold[c] = u;
-      } else {
-        uo = Uold[c];
-      }
-      u.a = c0 * uo.a + c1 * (u.a + dt * (a0));
-      u.b = c0 * uo.b + c1 * (u.b + dt * (a1));
-      u.c = c0 * uo.c + c1 * (u.c + dt * (a2));
-      u.d = c0 * uo.d + c1 * (u.d + dt * (a3));
-      U[c] = u;
-    }
-  }
+  if (c < nc) r2 = cell_residual_at<T, kRk>(c, nc, slot, g, F, etq, etqy, U, Uold, R, rk);
   if (kRk && rk.norm_part) {
     const double s = block_sum(r2, smem);
     if (threadIdx.x == 0) rk.norm_part[blockIdx.x] = s;

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "step.cuh"
 
 namespace o2f {
 
@@ -69,26 +70,11 @@ __device__ bool grid_reduce(double (&v)[N], double* part, unsigned int* ticket, 
 }
 
 // ---------------------------------------------------------------------------
-// Time-step control of Simulator::time_loop (src/simulation.cpp:68-124).
-
-struct StepState {
-  double t, dt, final_time, cfl, min_h, mu;
-  double hist0, drop_tol;
-  unsigned long long max_wave_bits;  // max(|u|+c) as the bits of a positive double
-  long long step, max_steps;
-  int stop;  // 0 running, 1 finished (time, step cap or residual drop), 2 non-finite
-  int drop_hit;
-};
+// Time-step control of Simulator::time_loop (src/simulation.cpp:68-124); the
+// per-step device functions and StepState are in step.cuh.
 
 // Start of a step: evaluate the loop condition, reset the wave-speed maximum.
-__global__ void k_step_begin(StepState* st) {
-  if (st->stop) return;
-  if (!(st->t < st->final_time) || st->step >= st->max_steps || st->drop_hit) {
-    st->stop = 1;
-    return;
-  }
-  st->max_wave_bits = (unsigned long long)__double_as_longlong(1e-8);
-}
+__global__ void k_step_begin(StepState* st) { step_begin_at(st); }
 
 // max over cells of hypot(u, v) + c (src/simulation.cpp:80-96).  The maximum
 // of positive doubles is exact, so the atomic order does not matter.
@@ -98,65 +84,21 @@ __global__ void __launch_bounds__(kBlock) k_wave_speed(int64_t nc, const Vec4<T>
   if (st->stop) return;
   double m = 0.0;
   bool bad = false;  // a non-finite speed anywhere stops the loop
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-    const Vec4<T> q = U[c];
-    const double rho = q.a, ru = q.b, rv = q.c, E = q.d;
-    const double u = ru / rho, v = rv / rho;
-    const double kinetic = 0.5 * (ru * ru + rv * rv) / rho;
-    const double p = (gamma - 1.0) * (E - kinetic);
-    const double cs = sqrt(gamma * p / rho);
-    const double speed = hypot(u, v) + cs;
-    if (!(speed <= 1.7976931348623157e308)) bad = true;  // NaN or +inf
-    else if (speed > m) m = speed;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    const double other = __shfl_down_sync(0xffffffffu, m, o);
-    if (other > m) m = other;
-  }
-  bad = __any_sync(0xffffffffu, bad);
-  if ((threadIdx.x & 31) == 0) {
-    if (bad) {
-      atomicExch(&st->stop, 2);
-    } else if (m > 0.0) {
-      atomicMax(&st->max_wave_bits, (unsigned long long)__double_as_longlong(m));
-    }
-  }
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x)
+    wave_speed_cell(U[c], gamma, m, bad);
+  wave_speed_commit(m, bad, st);
 }
 
 // dt = min(CFL*min_h/max_wave, 0.5*min_h^2/mu) (src/simulation.cpp:108-110).
-__global__ void k_step_dt(StepState* st) {
-  if (st->stop) return;
-  const double max_wave = __longlong_as_double((long long)st->max_wave_bits);
-  const double dt_adv = st->cfl * st->min_h / max_wave;
-  const double dt_diff = 0.5 * (st->min_h * st->min_h) / st->mu;
-  st->dt = smin(dt_adv, dt_diff);
-}
+__global__ void k_step_dt(StepState* st) { step_dt_at(st); }
 
 // Residual history: ||R_rho||_2 of the first stage, from the per-block partials.
 __global__ void k_step_norm(const double* part, int nparts, double* hist, StepState* st) {
   if (st->stop) return;
-  __shared__ double sm[32];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double tot = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sm[w];
-    const double nrm = sqrt(tot);
-    if (hist) hist[st->step] = nrm;
-    if (st->step == 0) st->hist0 = nrm;
-    if (!(nrm <= 1.7976931348623157e308)) st->stop = 2;  // NaN or +inf
-    if (st->drop_tol > 0.0 && st->hist0 > 0.0 && nrm <= st->drop_tol * st->hist0) st->drop_hit = 1;
-  }
+  step_norm_block(part, nparts, hist, st);
 }
 
-__global__ void k_step_end(StepState* st) {
-  if (st->stop) return;
-  st->t += st->dt;
-  st->step += 1;
-}
+__global__ void k_step_end(StepState* st) { step_end_at(st); }
 
 // ---------------------------------------------------------------------------
 // computeLiftDragCoefficients (src/compute.cpp:92-132) and

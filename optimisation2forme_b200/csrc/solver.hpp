@@ -42,7 +42,11 @@ class DeviceArena {
   size_t bytes_ = 0;
 };
 
+class Batch;
+
 class Solver {
+  friend class Batch;  // the batched time loop drives the context's device state (batch.cu)
+
  public:
   Solver(const o2f_mesh_desc& desc, const o2f_params& p, cudaStream_t stream);
   ~Solver();

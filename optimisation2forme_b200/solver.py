@@ -441,6 +441,59 @@ class Solver:
         return {"residual_ms": t.residual_ms, "kernel_launches": t.kernel_launches}
 
 
+class Batch:
+    """Several FP64 Solver contexts advanced together by the batched time loop
+    (o2f_batch_*): one grouped launch per phase of each SSP-RK3 step for all
+    candidates, each candidate with its own mesh, flow parameters, dt and stop
+    condition, and the same FP64 states as Solver.time_loop.  The contexts must
+    outlive the batch."""
+
+    PHASES = ("vertex_state", "cell_gradient", "vertex_visc", "edge_flux", "cell_residual", "wave_speed")
+
+    def __init__(self, solvers: Sequence[Solver]):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = C.c_void_p()
+        check(lib().o2f_batch_create(arr, len(self.solvers), C.byref(h)))
+        self._h = h
+
+    def tune(self, reps: int = 5) -> dict:
+        """Autotune block size and entities per thread of every phase."""
+        cfg = (C.c_int * (2 * len(self.PHASES)))()
+        check(lib().o2f_batch_tune(self._h, int(reps), cfg))
+        return {p: (cfg[2 * i], cfg[2 * i + 1]) for i, p in enumerate(self.PHASES)}
+
+    def time_loop(self, max_steps: int, residual_drop: float = 0.0) -> list[dict]:
+        n = len(self.solvers)
+        steps = (C.c_int64 * n)()
+        t = np.zeros(n)
+        st = (C.c_int * n)()
+        check(lib().o2f_batch_rk3_run(self._h, int(max_steps), float(residual_drop), steps, _ptr(t), st))
+        return [{"steps": steps[i], "t": float(t[i]), "status": _lib.STATUS.get(st[i], "OK")} for i in range(n)]
+
+    def history(self, index: int, count: int) -> np.ndarray:
+        out = np.empty(max(int(count), 1))
+        check(lib().o2f_batch_history(self._h, int(index), _ptr(out), int(count)))
+        return out[: int(count)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib().o2f_batch_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def write_shape_log(path: str | os.PathLike, names: Sequence[str], J: float, grad: Sequence[float]) -> None:
     """appendShapeOptLog (src/shape_optimization.cpp:112-145): the file is
     truncated and holds one line `` J=<%.8f> name=<%.6e> ...``."""

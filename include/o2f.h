@@ -222,6 +222,12 @@ int o2f_adjoint_rhs(o2f_ctx* ctx, double beta, double* b_host);
 int o2f_adjoint_solve(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, int64_t restart,
                       double* lambda_host, int64_t* iters, double* relres);
 
+/* NEW: o2f_adjoint_solve started from lambda0_host (reference order)
+ * instead of zero -- the warm start of the learned predictor.  The solution
+ * criterion is unchanged: true relres <= tol. */
+int o2f_adjoint_solve_guess(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, int64_t restart,
+                            const double* lambda0_host, double* lambda_host, int64_t* iters, double* relres);
+
 /* NACA-4 shape parameters (src/shape_optimization.cpp:830-834 defaults). */
 typedef struct o2f_shape_params {
   double pos_x; /* 0.355 */
@@ -310,6 +316,33 @@ int o2f_batch_rk3_run(o2f_batch* batch, int64_t max_steps, double drop_tol, int6
                       int* status_out);
 /* ||R_rho||_2 history of candidate `index` from the last o2f_batch_rk3_run. */
 int o2f_batch_history(o2f_batch* batch, int index, double* history_host, int64_t count);
+
+/* Warm-start network (no reference counterpart).  Inputs per point:
+ * {x, y, m, p, t, Mach, AoA} (float32, 7 per point); outputs: 8 float32
+ * (normalised state and adjoint, as the caller defines them).  Fourier
+ * features of (x, y) (32 seeded frequencies, scale freq_scale) and the raw
+ * inputs feed 4 hidden layers of 256 SiLU units.  Training (MSE, Adam) and
+ * inference run on the GPU in this library's tcgen05 kernels: BF16 weights
+ * and activations, FP32 accumulation, FP32 master weights.  max_batch bounds
+ * the points per GEMM pass (128 .. 2^20). */
+typedef struct o2f_mlp o2f_mlp;
+int o2f_mlp_create(int max_batch, float freq_scale, uint64_t seed, void* stream, o2f_mlp** out);
+int o2f_mlp_destroy(o2f_mlp* net);
+int o2f_mlp_n_params(o2f_mlp* net, int64_t* n);
+/* Copies a training set to the device: inputs [n*7], targets [n*8]. */
+int o2f_mlp_set_data(o2f_mlp* net, const float* inputs, const float* targets, int64_t n);
+/* `steps` Adam steps on seeded minibatches of `batch` points; loss_history
+ * (may be NULL) receives the minibatch MSE of each step. */
+int o2f_mlp_train(o2f_mlp* net, int steps, int batch, float lr, uint64_t seed, float* loss_history);
+int o2f_mlp_predict(o2f_mlp* net, const float* inputs, int64_t n, float* outputs);
+/* Gradient of the MSE on one batch (n <= max_batch) without an update:
+ * grads [o2f_mlp_n_params] in the parameter layout W0,b0,...,W4,b4 (W_l
+ * row-major [out][in]; layer sizes 128->256->256->256->256->16, outputs 8..15
+ * are padding and stay zero). */
+int o2f_mlp_gradients(o2f_mlp* net, const float* inputs, const float* targets, int n, float* grads, float* loss);
+/* Parameters (same layout) and the Fourier frequencies [64] (may be NULL). */
+int o2f_mlp_get_params(o2f_mlp* net, float* params, float* freq);
+int o2f_mlp_set_params(o2f_mlp* net, const float* params);
 
 /* No counterpart in the reference.  Residual of the current state (as
  * o2f_residual, interface states left in the context) and its

@@ -98,6 +98,7 @@ class Timing(C.Structure):
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int64)
 _vp = C.c_void_p
+_fp = C.POINTER(C.c_float)
 
 # name -> (argtypes); every function returns int except noted.
 SIGNATURES = {
@@ -135,6 +136,17 @@ SIGNATURES = {
     "o2f_profile_kernels": ([_vp, C.c_int, _dp], C.c_int),
     "o2f_residual_norm_noalloc": ([_vp, _dp], C.c_int),
     "o2f_batch_create": ([C.POINTER(_vp), C.c_int, C.POINTER(_vp)], C.c_int),
+    "o2f_adjoint_solve_guess": ([_vp, C.c_double, C.c_double, C.c_int64, C.c_int64, _dp, _dp, C.POINTER(C.c_int64),
+                                 _dp], C.c_int),
+    "o2f_mlp_create": ([C.c_int, C.c_float, C.c_uint64, _vp, C.POINTER(_vp)], C.c_int),
+    "o2f_mlp_destroy": ([_vp], C.c_int),
+    "o2f_mlp_n_params": ([_vp, C.POINTER(C.c_int64)], C.c_int),
+    "o2f_mlp_set_data": ([_vp, _fp, _fp, C.c_int64], C.c_int),
+    "o2f_mlp_train": ([_vp, C.c_int, C.c_int, C.c_float, C.c_uint64, _fp], C.c_int),
+    "o2f_mlp_predict": ([_vp, _fp, C.c_int64, _fp], C.c_int),
+    "o2f_mlp_gradients": ([_vp, _fp, _fp, C.c_int, _fp, _fp], C.c_int),
+    "o2f_mlp_get_params": ([_vp, _fp, _fp], C.c_int),
+    "o2f_mlp_set_params": ([_vp, _fp], C.c_int),
     "o2f_batch_destroy": ([_vp], C.c_int),
     "o2f_batch_tune": ([_vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "o2f_batch_rk3_run": ([_vp, C.c_int64, C.c_double, C.POINTER(C.c_int64), _dp, C.POINTER(C.c_int)], C.c_int),

@@ -33,6 +33,21 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libo2f.so")
 
 
+def _cutlass_include() -> str:
+    """CUTLASS/CuTe headers (the tcgen05 descriptor layouts of the warm-start
+    GEMM): $O2F_CUTLASS_INCLUDE, else the copy vendored with flashinfer."""
+    import importlib.util
+    env = os.environ.get("O2F_CUTLASS_INCLUDE")
+    if env and (Path(env) / "cute").is_dir():
+        return env
+    spec = importlib.util.find_spec("flashinfer")
+    for loc in (spec.submodule_search_locations or []) if spec else []:
+        cand = Path(loc) / "data" / "cutlass" / "include"
+        if (cand / "cute" / "arch" / "mma_sm100_desc.hpp").exists():
+            return str(cand)
+    raise RuntimeError("CUTLASS headers not found: set O2F_CUTLASS_INCLUDE to a CUTLASS include directory")
+
+
 def _deps(src: Path) -> list[Path]:
     return [src] + sorted(CSRC.glob("*.hpp")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "o2f.h"]
 
@@ -70,10 +85,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     for src in sorted(CSRC.glob("*.cu")):
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
-        fmad = "-fmad=false" if not src.stem.endswith("_f32") else "-fmad=true"
+        # FP64 parity code: no FMA contraction.  Mixed-precision and network
+        # code: contraction on; the network also needs the CUTLASS headers.
+        learned = src.stem.startswith("mlp")
+        fmad = "-fmad=true" if src.stem.endswith("_f32") or learned else "-fmad=false"
+        extra = [f"-I{_cutlass_include()}"] if learned else []
         if force or _stale(obj, _deps(src)):
             jobs.append([nvcc, *ARCH, "-O3", "-std=c++17", "-lineinfo", fmad, "--expt-relaxed-constexpr",
-                         "-Xcompiler", "-fPIC,-ffp-contract=off", *inc, "-c", str(src), "-o", str(obj)])
+                         "-Xcompiler", "-fPIC,-ffp-contract=off", *inc, *extra, "-c", str(src), "-o", str(obj)])
     procs = []
     for cmd in jobs:
         if verbose:

@@ -11,6 +11,7 @@
 
 #include "batch.hpp"
 #include "mesh_host.hpp"
+#include "mlp.hpp"
 #include "o2f.h"
 #include "solver.hpp"
 
@@ -24,6 +25,10 @@ struct o2f_host_mesh {
 
 struct o2f_batch {
   std::unique_ptr<o2f::Batch> batch;
+};
+
+struct o2f_mlp {
+  std::unique_ptr<o2f::mlp::Mlp> net;
 };
 
 namespace {
@@ -267,6 +272,14 @@ int o2f_adjoint_solve(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, i
   return guarded([&] { S(ctx).adjoint_solve(beta, tol, max_iter, restart, lambda_host, iters, relres); });
 }
 
+int o2f_adjoint_solve_guess(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, int64_t restart,
+                            const double* lambda0_host, double* lambda_host, int64_t* iters, double* relres) {
+  return guarded([&] {
+    need(lambda0_host, "lambda0");
+    S(ctx).adjoint_solve(beta, tol, max_iter, restart, lambda_host, iters, relres, lambda0_host);
+  });
+}
+
 int o2f_shape_gradient(o2f_ctx* ctx, const o2f_shape_params* shape, const int* param_ids, int n_params, double beta,
                        double eps, const double* lambda_host, double* grad_out) {
   return guarded([&] {
@@ -362,6 +375,77 @@ int o2f_batch_history(o2f_batch* batch, int index, double* history_host, int64_t
   return guarded([&] {
     need(history_host, "history");
     B(batch).history(index, history_host, count);
+  });
+}
+
+namespace {
+o2f::mlp::Mlp& N(o2f_mlp* m) {
+  if (!m || !m->net) throw o2f::Error(O2F_ERR_ARG, "null network");
+  return *m->net;
+}
+}  // namespace
+
+int o2f_mlp_create(int max_batch, float freq_scale, uint64_t seed, void* stream, o2f_mlp** out) {
+  return guarded([&] {
+    need(out, "out");
+    *out = nullptr;
+    auto m = std::make_unique<o2f_mlp>();
+    m->net = std::make_unique<o2f::mlp::Mlp>(max_batch, freq_scale, seed, static_cast<cudaStream_t>(stream));
+    *out = m.release();
+  });
+}
+
+int o2f_mlp_destroy(o2f_mlp* net) {
+  return guarded([&] { delete net; });
+}
+
+int o2f_mlp_n_params(o2f_mlp* net, int64_t* n) {
+  return guarded([&] {
+    need(n, "n");
+    *n = N(net).n_params();
+  });
+}
+
+int o2f_mlp_set_data(o2f_mlp* net, const float* inputs, const float* targets, int64_t n) {
+  return guarded([&] {
+    need(inputs, "inputs");
+    need(targets, "targets");
+    N(net).set_data(inputs, targets, n);
+  });
+}
+
+int o2f_mlp_train(o2f_mlp* net, int steps, int batch, float lr, uint64_t seed, float* loss_history) {
+  return guarded([&] { N(net).train(steps, batch, lr, seed, loss_history); });
+}
+
+int o2f_mlp_predict(o2f_mlp* net, const float* inputs, int64_t n, float* outputs) {
+  return guarded([&] {
+    need(inputs, "inputs");
+    need(outputs, "outputs");
+    N(net).predict(inputs, n, outputs);
+  });
+}
+
+int o2f_mlp_gradients(o2f_mlp* net, const float* inputs, const float* targets, int n, float* grads, float* loss) {
+  return guarded([&] {
+    need(inputs, "inputs");
+    need(targets, "targets");
+    need(grads, "grads");
+    N(net).gradients(inputs, targets, n, grads, loss);
+  });
+}
+
+int o2f_mlp_get_params(o2f_mlp* net, float* params, float* freq) {
+  return guarded([&] {
+    need(params, "params");
+    N(net).get_params(params, freq);
+  });
+}
+
+int o2f_mlp_set_params(o2f_mlp* net, const float* params) {
+  return guarded([&] {
+    need(params, "params");
+    N(net).set_params(params);
   });
 }
 

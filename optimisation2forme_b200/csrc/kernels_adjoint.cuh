@@ -83,10 +83,9 @@ __global__ void __launch_bounds__(kBlock) k_wave_speed(int64_t nc, const Vec4<T>
                                                        StepState* st) {
   if (st->stop) return;
   double m = 0.0;
-  bool bad = false;  // a non-finite speed anywhere stops the loop
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x)
-    wave_speed_cell(U[c], gamma, m, bad);
-  wave_speed_commit(m, bad, st);
+    wave_speed_cell(U[c], gamma, m);
+  wave_speed_commit(m, st);
 }
 
 // dt = min(CFL*min_h/max_wave, 0.5*min_h^2/mu) (src/simulation.cpp:108-110).

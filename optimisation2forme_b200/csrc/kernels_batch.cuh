@@ -77,12 +77,11 @@ __global__ void __launch_bounds__(kBatchMaxBlock) kb_wave_speed(const BatchItem*
   if (*(volatile const int*)&it.st->stop) return;
   const int64_t base = (int64_t)(blockIdx.x - off[i]) * blockDim.x * tile + threadIdx.x;
   double m = 0.0;
-  bool bad = false;
   for (int k = 0; k < tile; ++k) {
     const int64_t c = base + (int64_t)k * blockDim.x;
-    if (c < it.t.nc) wave_speed_cell(it.U[c], it.ph.gamma, m, bad);
+    if (c < it.t.nc) wave_speed_cell(it.U[c], it.ph.gamma, m);
   }
-  wave_speed_commit(m, bad, it.st);
+  wave_speed_commit(m, it.st);
 }
 
 // Scalar steps: one thread per candidate.

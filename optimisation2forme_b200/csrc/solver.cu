@@ -870,7 +870,7 @@ void Solver::adjoint_rhs(double beta, double* b_ref) {
 }
 
 void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
-                           int64_t* iters, double* relres_out) {
+                           int64_t* iters, double* relres_out, const double* guess_ref) {
   if (!(tol > 0.0) || max_iter <= 0 || restart <= 0) throw Error(O2F_ERR_ARG, "invalid solver settings");
   build_jt_blocks();
   adjoint_rhs(beta, nullptr);
@@ -887,7 +887,10 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   need(t_);
   need(tmp_);
   double* x = reinterpret_cast<double*>(lam_);
-  O2F_CUDA(cudaMemsetAsync(lam_, 0, nc * sizeof(Vec4<double>), stream_));
+  if (guess_ref)  // warm start: the first chunk's residual is b - J^T lambda0
+    to_internal(guess_ref, lam_);
+  else
+    O2F_CUDA(cudaMemsetAsync(lam_, 0, nc * sizeof(Vec4<double>), stream_));
   // ||b||^2
   k_dot2<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_), reinterpret_cast<double*>(b_), nullptr,
                                            nullptr, part_, ticket_, scal_);
@@ -901,13 +904,21 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   double relres = INFINITY;
   // Right-preconditioned BiCGSTAB: phat = M^{-1} p, shat = M^{-1} s; the
   // recurrence residual r stays the true residual of J^T lambda = b.
-  const bool precond = params_.adjoint_precond == O2F_PRECOND_ILU0;
+  bool precond = params_.adjoint_precond == O2F_PRECOND_ILU0;
   Vec4<double>* ph = p_;
   Vec4<double>* sh = s_;
   if (precond) {
-    ilu_factor();
-    ph = phat_;
-    sh = shat_;
+    try {
+      ilu_factor();
+      ph = phat_;
+      sh = shat_;
+    } catch (const Error& e) {
+      // A singular diagonal block (e.g. a cell whose pressure went negative):
+      // this solve runs the reference's identity-preconditioned iteration.
+      if (e.code != O2F_ERR_BREAKDOWN) throw;
+      precond = false;
+      if (params_.verbosity >= 1) std::fprintf(stderr, "[adjoint] ILU(0) breakdown: identity preconditioner\n");
+    }
   }
   const int kItersPerGraph = precond ? 1 : 8;
   const int kernels_per_iter = 5 + (precond ? 4 : 0);

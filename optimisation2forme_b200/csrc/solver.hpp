@@ -68,7 +68,7 @@ class Solver {
   void jt_apply(const double* x_ref, double* y_ref);
   void adjoint_rhs(double beta, double* b_ref);
   void adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
-                     int64_t* iters, double* relres);
+                     int64_t* iters, double* relres, const double* guess_ref = nullptr);
   void shape_gradient(const o2f_shape_params& sp, const int* ids, int n, double beta, double eps,
                       const double* lambda_ref, double* grad);
   void debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which, double* out);

@@ -25,33 +25,30 @@ __device__ __forceinline__ void step_begin_at(StepState* st) {
   }
   st->max_wave_bits = (unsigned long long)__double_as_longlong(1e-8);
 }
-// |u| + c of one cell state; `bad` set for a non-finite speed.
+// |u| + c of one cell state folded into the running maximum m with the
+// reference's std::max(max_wave, speed) semantics (src/simulation.cpp:96): a
+// NaN speed (a cell whose pressure or density went negative while its
+// interface states stayed valid) is skipped, not fatal.  Non-finite states
+// and residuals are caught by the residual norm (step_norm_block).
 template <typename T>
-__device__ __forceinline__ void wave_speed_cell(const Vec4<T>& q, double gamma, double& m, bool& bad) {
+__device__ __forceinline__ void wave_speed_cell(const Vec4<T>& q, double gamma, double& m) {
   const double rho = q.a, ru = q.b, rv = q.c, E = q.d;
   const double u = ru / rho, v = rv / rho;
   const double kinetic = 0.5 * (ru * ru + rv * rv) / rho;
   const double p = (gamma - 1.0) * (E - kinetic);
   const double cs = sqrt(gamma * p / rho);
   const double speed = hypot(u, v) + cs;
-  if (!(speed <= 1.7976931348623157e308)) bad = true;  // NaN or +inf
-  else if (speed > m) m = speed;
+  if (speed > m) m = speed;
 }
 
 // Warp-level combination of the per-thread maxima into st.
-__device__ __forceinline__ void wave_speed_commit(double m, bool bad, StepState* st) {
+__device__ __forceinline__ void wave_speed_commit(double m, StepState* st) {
   for (int o = 16; o > 0; o >>= 1) {
     const double other = __shfl_down_sync(0xffffffffu, m, o);
     if (other > m) m = other;
   }
-  bad = __any_sync(0xffffffffu, bad);
-  if ((threadIdx.x & 31) == 0) {
-    if (bad) {
-      atomicExch(&st->stop, 2);
-    } else if (m > 0.0) {
-      atomicMax(&st->max_wave_bits, (unsigned long long)__double_as_longlong(m));
-    }
-  }
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(&st->max_wave_bits, (unsigned long long)__double_as_longlong(m));
 }
 
 // dt = min(CFL*min_h/max_wave, 0.5*min_h^2/mu) (src/simulation.cpp:108-110).

@@ -355,13 +355,21 @@ class Solver:
         return b
 
     def solve_adjoint_system(self, beta: float = 1.0, tol: float = 1e-6, max_iter: int = 100000,
-                             restart: int = 500, raise_on_failure: bool = True) -> dict:
-        """solveAdjointSystem (src/shape_optimization.cpp:658-740)."""
+                             restart: int = 500, raise_on_failure: bool = True, guess: np.ndarray | None = None) -> dict:
+        """solveAdjointSystem (src/shape_optimization.cpp:658-740); `guess`
+        (reference order, 4 per cell) replaces the zero initial lambda."""
         lam = np.empty(4 * self.n_cells)
         it = C.c_int64()
         rr = C.c_double()
-        code = lib().o2f_adjoint_solve(self._h, float(beta), float(tol), int(max_iter), int(restart), _ptr(lam),
-                                       C.byref(it), C.byref(rr))
+        if guess is None:
+            code = lib().o2f_adjoint_solve(self._h, float(beta), float(tol), int(max_iter), int(restart), _ptr(lam),
+                                           C.byref(it), C.byref(rr))
+        else:
+            g = np.ascontiguousarray(guess, dtype=np.float64).reshape(-1)
+            if g.size != 4 * self.n_cells:
+                raise ValueError("guess must hold 4 values per cell")
+            code = lib().o2f_adjoint_solve_guess(self._h, float(beta), float(tol), int(max_iter), int(restart),
+                                                 _ptr(g), _ptr(lam), C.byref(it), C.byref(rr))
         res = {"lambda": lam, "iters": it.value, "relres": rr.value, "status": _lib.STATUS.get(code, "OK")}
         if code != 0 and raise_on_failure:
             check(code)

@@ -59,6 +59,23 @@ def naca_name(spec) -> str:
     return f"{m}{p}{int(round(spec.t * 100)):02d}"
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The largest of every rank's x (each rank times its own replica; the
+    job takes as long as the slowest).  world == 1: x itself."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, evals_per_rank: int, seconds: float) -> float:
+    """Whole-job evaluations per second: every rank evaluates its own
+    candidate (weak scaling), timed by the slowest rank."""
+    return world * evals_per_rank / seconds
+
+
 def load_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -209,12 +226,8 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
         torch.cuda.synchronize()
     launches = s.timing()["kernel_launches"] - launches0
     barrier()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    value = replica_throughput(world, args.steps, ms / 1e3)
 
     # End to end through the C ABI with host buffers: the initial state goes
     # host->device (pinned) each step, the final state and the gradient come back.
@@ -231,12 +244,8 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
             adjoint_and_gradient()
             Uf = s.get_state()
         torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([dt], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            dt = float(t.item())
-        e2e = {"value": world * args.e2e_steps / dt, "unit": "evals/s", "h2d_bytes_per_step": int(U0.nbytes),
+        dt = max_over_ranks(time.perf_counter() - t0, world)
+        e2e = {"value": replica_throughput(world, args.e2e_steps, dt), "unit": "evals/s", "h2d_bytes_per_step": int(U0.nbytes),
                "d2h_bytes_per_step": int(Uf.nbytes + 8 * s.n_cells * 4 + 8 * len(names) + 24)}
 
     # Per-kernel launch durations (CUDA events on the solver's stream) about

@@ -414,162 +414,6 @@ __global__ void __launch_bounds__(kBlock) k_cell_gradient(
   cell_gradient_at<T, kWriteGrad>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad);
 }
 
-// K2 with four lanes per cell: lane q of a quad carries conserved variable q
-// (rho, rho_u, rho_v, E) through the edge values, the Green-Gauss sums, the
-// neighbour min/max, the limiter and the interface states -- the same
-// operations on the same values as cell_gradient_at, so the results are
-// bit-identical -- and the quad exchanges by shuffles what couples the
-// variables: the wall state of bc_state (rho, rho_u, rho_v) and the viscous
-// stresses (every gradient).  Four times the threads of the one-lane kernel
-// at about half its registers, which hides the gather latency.
-template <typename T>
-__device__ __forceinline__ T fs_component(const Phys& ph, int q) {
-  return (T)(q == 0 ? ph.fs_rho : q == 1 ? ph.fs_rhou : q == 2 ? ph.fs_rhov : ph.fs_E);
-}
-
-template <typename T, bool kWriteGrad>
-__global__ void __launch_bounds__(kBlock, 4) k_cell_gradient4(
-    int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
-    const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
-    const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
-    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad, const int* gate) {
-  if (gated(gate)) return;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t c = t >> 2;
-  if (c >= nc) return;  // the four lanes of a cell leave together
-  const int q = (int)(t & 3);
-  const unsigned qmask = 0xFu << (threadIdx.x & 28u);
-  const T* __restrict__ Uq = reinterpret_cast<const T*>(U);
-  const T* __restrict__ vqq = reinterpret_cast<const T*>(vq);
-  const Vec4<T> cg = g.cgeom[c];
-  const T cx = cg.a, cy = cg.b, cv = cg.c, veps = cg.d;
-  const T u = Uq[4 * c + q];
-  int sl[4], nk = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) sl[k] = slot[(int64_t)k * nc + c];
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (sl[k] >= 0 && nk == k) nk = k + 1;
-  int2 evv[4], cc[4];
-  uint8_t code[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k < nk) {
-      const int e = sl[k] >> 1;
-      evv[k] = ev[e];
-      cc[k] = ec[e];
-      code[k] = ebc[e];
-    }
-  }
-  T gx = (T)0.0, gy = (T)0.0, mn = u, mx = u;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k >= nk) continue;
-    const int s = sl[k];
-    const int e = s >> 1;
-    const bool left = (s & 1) == 0;
-    const T va = vqq[4 * (int64_t)evv[k].x + q], vb = vqq[4 * (int64_t)evv[k].y + q];
-    const Vec4<T> eg = g.egeom[e];
-    const int o = left ? cc[k].y : cc[k].x;
-    T un = u;
-    if (o >= 0) un = Uq[4 * (int64_t)o + q];
-    T er = (T)0.5 * (va + vb);
-    const uint8_t cd = code[k];
-    if (cd == 'i' || cd == 'f') {
-      er = fs_component<T>(ph, q);
-    } else if (cd == 'w') {  // bc_state: keep rho and the internal energy, zero momentum
-      const T r = __shfl_sync(qmask, er, 0, 4);
-      const T ru = __shfl_sync(qmask, er, 1, 4);
-      const T rv = __shfl_sync(qmask, er, 2, 4);
-      if (q == 1 || q == 2) {
-        er = (T)0.0;
-      } else if (q == 3) {
-        const T kinetic_old = (T)0.5 * (ru * ru + rv * rv) / r;
-        er = er - kinetic_old;
-      }
-    }
-    const T el = eg.c;
-    T enx = eg.a, eny = eg.b;
-    if (left) {
-      enx = -enx;
-      eny = -eny;
-    }
-    gx += er * el * enx / cv;
-    gy += er * el * eny / cv;
-    if (o >= 0) {
-      if (un < mn) mn = un;
-      if (un > mx) mx = un;
-    }
-  }
-  const int kind = ph.limiter;
-  T al = (T)1.0;
-  T dxk[4], dyk[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k >= nk) continue;
-    const Vec2<T> ce = g.ectr[sl[k] >> 1];
-    const T dx = ce.a - cx, dy = ce.b - cy;
-    dxk[k] = dx;
-    dyk[k] = dy;
-    al = smin(al, limiter_alpha(kind, u, u + gx * dx + gy * dy, mn, mx, veps));
-  }
-  T* __restrict__ eLq = reinterpret_cast<T*>(eL);
-  T* __restrict__ eRq = reinterpret_cast<T*>(eR);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k >= nk) continue;
-    const int s = sl[k];
-    const int64_t e = s >> 1;
-    const T st = u + al * (gx * dxk[k] + gy * dyk[k]);
-    if ((s & 1) == 0) {
-      eLq[4 * e + q] = st;
-      const uint8_t cd = code[k];
-      if (cd) {  // bc_ghost
-        T gh = st;
-        if (cd == 'i' || cd == 'f') gh = fs_component<T>(ph, q);
-        else if (cd == 'w' && (q == 1 || q == 2)) gh = -st;
-        eRq[4 * e + q] = gh;
-      }
-    } else {
-      eRq[4 * e + q] = st;
-    }
-  }
-  // Viscous stress and heat flux at the cell (src/diffusion.cpp:227-240).
-  const T gx0 = __shfl_sync(qmask, gx, 0, 4), gx1 = __shfl_sync(qmask, gx, 1, 4);
-  const T gx2 = __shfl_sync(qmask, gx, 2, 4), gx3 = __shfl_sync(qmask, gx, 3, 4);
-  const T gy0 = __shfl_sync(qmask, gy, 0, 4), gy1 = __shfl_sync(qmask, gy, 1, 4);
-  const T gy2 = __shfl_sync(qmask, gy, 2, 4), gy3 = __shfl_sync(qmask, gy, 3, 4);
-  const T ua = __shfl_sync(qmask, u, 0, 4), ub = __shfl_sync(qmask, u, 1, 4);
-  const T uc = __shfl_sync(qmask, u, 2, 4), ud = __shfl_sync(qmask, u, 3, 4);
-  const T mu = (T)ph.mu, gamma = (T)ph.gamma, kappa = (T)ph.kappa;
-  const T uu = ub / ua;
-  const T vv = uc / ua;
-  const T u_x = (gx1 - uu * gx0) / ua;
-  const T v_y = (gy2 - vv * gy0) / ua;
-  const T u_y = (gy1 - uu * gy0) / ua;
-  const T v_x = (gx2 - vv * gx0) / ua;
-  const T two_thirds = (T)(2.0 / 3.0);
-  T out;
-  if (q == 0) {
-    out = (T)2 * mu * u_x - two_thirds * mu * (u_x + v_y);
-  } else if (q == 1) {
-    out = (T)2 * mu * v_y - two_thirds * mu * (u_x + v_y);
-  } else if (q == 2) {
-    out = mu * (u_y + v_x);
-  } else {
-    const T T_x = (gamma - (T)1.0) * ((gx3 * ua - ud * gx0) / (ua * ua) - (uu * u_x + vv * v_x));
-    const T T_y = (gamma - (T)1.0) * ((gy3 * ua - ud * gy0) / (ua * ua) - (uu * u_y + vv * v_y));
-    out = -kappa * T_x;
-    ctqy[c] = -kappa * T_y;
-  }
-  reinterpret_cast<T*>(ctq)[4 * c + q] = out;
-  if (kWriteGrad) {
-    T* gq = reinterpret_cast<T*>(grad);
-    gq[8 * c + q] = gx;
-    gq[8 * c + 4 + q] = gy;
-  }
-}
-
 // K4: per edge -- HLLC flux (src/advection.cpp:433-437) and the edge viscous
 // quantities with their boundary conditions (src/diffusion.cpp:145-170).
 template <typename T>

@@ -575,10 +575,10 @@ void Solver::launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<
   cudaStream_t s = stream_;
   k_vertex_state<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, U, phys_, w.vq, gate);
   if (write_grad)
-    k_cell_gradient4<double, true><<<grid(4 * t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
+    k_cell_gradient<double, true><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
                                                                 w.eL, w.eR, w.ctq, w.ctqy, w.grad, gate);
   else
-    k_cell_gradient4<double, false><<<grid(4 * t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
+    k_cell_gradient<double, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
                                                                  w.eL, w.eR, w.ctq, w.ctqy, w.grad, gate);
   k_vertex_visc<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, w.ctq, w.ctqy, w.vtq,
                                                       w.vtqy, gate);
@@ -639,7 +639,7 @@ void Solver::profile_kernels(int reps, double* ms_out) {
                                                                nullptr);
           break;
         case O2F_K_CELL_GRADIENT:
-          k_cell_gradient4<double, false><<<grid(4 * t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U_, w.vq,
+          k_cell_gradient<double, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U_, w.vq,
                                                                        phys_, w.eL, w.eR, w.ctq, w.ctqy, w.grad,
                                                                        nullptr);
           break;

@@ -90,7 +90,7 @@ void Solver::launch_residual_f32(const int* gate, const void* rkp) {
   const Work<float>& w = work32_;
   cudaStream_t s = stream_;
   k_vertex_state<float><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, U32_, phys_, w.vq, gate);
-  k_cell_gradient4<float, false><<<grid(4 * t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U32_, w.vq, phys_,
+  k_cell_gradient<float, false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U32_, w.vq, phys_,
                                                               w.eL, w.eR, w.ctq, w.ctqy, w.grad, gate);
   k_vertex_visc<float><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, w.ctq, w.ctqy, w.vtq, w.vtqy,
                                                      gate);

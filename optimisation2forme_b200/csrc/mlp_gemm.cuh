@@ -83,35 +83,61 @@ __device__ __forceinline__ uint64_t kmajor_desc(uint32_t chunk_addr, int rows, i
 }
 
 // Copy rows [r0, r0 + rows) x K chunk [k0, k0 + kKC) of X(r, k) into the
-// canonical layout; out-of-range elements are zero.
+// canonical layout; out-of-range elements are zero.  Row-contiguous operands
+// (k stride 1) go through cp.async, 16 bytes per copy, all in flight at once
+// (the caller waits with cp.async.wait_all); transposed operands are gathered
+// element by element, four 16-byte pieces per thread in flight.
+__device__ __forceinline__ void cp_async16(uint8_t* dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+
 __device__ __forceinline__ void fill_chunk(uint8_t* dst, int rows, const bf16* __restrict__ X, int64_t sr, int64_t sk,
                                            int r0, int rmax, int k0, int kmax) {
   const int groups = kKC / 8;
+  const int items = rows * groups;
   const bool contiguous = (sk == 1) && ((sr & 7) == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
-  for (int idx = threadIdx.x; idx < rows * groups; idx += blockDim.x) {
-    int r, g;
-    if (contiguous) {  // consecutive threads: consecutive 16-byte pieces of a row
-      r = idx / groups;
-      g = idx % groups;
-    } else {  // consecutive threads: consecutive rows (coalesced for transposed data)
-      r = idx % rows;
-      g = idx / rows;
-    }
-    const int gr = r0 + r, gk = k0 + g * 8;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (gr < rmax) {
-      if (contiguous && gk + 8 <= kmax) {
-        v = *reinterpret_cast<const uint4*>(X + (int64_t)gr * sr + gk);
-      } else {
+  if (contiguous) {
+    for (int idx = threadIdx.x; idx < items; idx += blockDim.x) {
+      const int r = idx / groups, g = idx % groups;  // consecutive threads: consecutive pieces of a row
+      const int gr = r0 + r, gk = k0 + g * 8;
+      uint8_t* p = dst + ((size_t)g * (rows / 8) + (r >> 3)) * 128 + (r & 7) * 16;
+      if (gk + 8 <= kmax || gk >= kmax) {
+        const bool valid = gr < rmax && gk < kmax;
+        cp_async16(p, valid ? (const void*)(X + (int64_t)gr * sr + gk) : (const void*)X, valid);
+      } else {  // a K edge inside the 8-element piece
         bf16 e[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-          e[j] = (gk + j < kmax) ? X[(int64_t)gr * sr + (int64_t)(gk + j) * sk] : __float2bfloat16_rn(0.f);
-        v = *reinterpret_cast<const uint4*>(e);
+          e[j] = (gr < rmax && gk + j < kmax) ? X[(int64_t)gr * sr + gk + j] : __float2bfloat16_rn(0.f);
+        *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(e);
       }
     }
-    uint8_t* p = dst + ((size_t)g * (rows / 8) + (r >> 3)) * 128 + (r & 7) * 16;
-    *reinterpret_cast<uint4*>(p) = v;
+    return;
+  }
+  constexpr int kBatch = 4;
+  for (int base = threadIdx.x; base < items; base += blockDim.x * kBatch) {
+    uint4 v[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {  // loads of kBatch pieces first
+      const int idx = base + u * blockDim.x;
+      const int r = idx % rows, g = idx / rows;  // consecutive threads: consecutive rows (coalesced)
+      const int gr = r0 + r, gk = k0 + g * 8;
+      bf16 e[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        e[j] = (idx < items && gr < rmax && gk + j < kmax) ? X[(int64_t)gr * sr + (int64_t)(gk + j) * sk]
+                                                          : __float2bfloat16_rn(0.f);
+      v[u] = *reinterpret_cast<const uint4*>(e);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx >= items) continue;
+      const int r = idx % rows, g = idx / rows;
+      *reinterpret_cast<uint4*>(dst + ((size_t)g * (rows / 8) + (r >> 3)) * 128 + (r & 7) * 16) = v[u];
+    }
   }
 }
 
@@ -170,7 +196,8 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs a) {
   for (int k0 = kb; k0 < ke; k0 += kKC) {
     fill_chunk(sA, kTileM, a.A, a.sam, a.sak, m0, a.M, k0, ke);
     fill_chunk(sB, NT, a.B, a.sbn, a.sbk, n0, a.N, k0, ke);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic smem writes -> tensor core
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // smem writes -> tensor core
     __syncthreads();
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -218,9 +245,42 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs a) {
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row >= a.M) continue;
+      const int nb = n0 + c0;
+      const int64_t o0 = (int64_t)row * a.ldo + nb;
+      // The thread's 16 consecutive outputs of its row go out as 16-byte
+      // vectors when the slice is whole and aligned (ldo a multiple of 8).
+      const bool whole = nb + 16 <= a.N && (a.ldo & 7) == 0;
+      if (a.epi == kEpiHidden && whole) {
+        alignas(16) bf16 zb[16], yb[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float z = __uint_as_float(r[j]) + (a.bias ? a.bias[nb + j] : 0.f);
+          zb[j] = __float2bfloat16_rn(z);
+          yb[j] = __float2bfloat16_rn(silu(z));
+        }
+        uint4* pz = reinterpret_cast<uint4*>(a.pre + o0);
+        uint4* py = reinterpret_cast<uint4*>(a.out + o0);
+        pz[0] = reinterpret_cast<const uint4*>(zb)[0];
+        pz[1] = reinterpret_cast<const uint4*>(zb)[1];
+        py[0] = reinterpret_cast<const uint4*>(yb)[0];
+        py[1] = reinterpret_cast<const uint4*>(yb)[1];
+        continue;
+      }
+      if (a.epi == kEpiBackAct && whole) {
+        alignas(16) bf16 zp[16], gb[16];
+        reinterpret_cast<uint4*>(zp)[0] = reinterpret_cast<const uint4*>(a.zprev + o0)[0];
+        reinterpret_cast<uint4*>(zp)[1] = reinterpret_cast<const uint4*>(a.zprev + o0)[1];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          gb[j] = __float2bfloat16_rn(__uint_as_float(r[j]) * silu_grad(__bfloat162float(zp[j])));
+        uint4* pg = reinterpret_cast<uint4*>(a.out + o0);
+        pg[0] = reinterpret_cast<const uint4*>(gb)[0];
+        pg[1] = reinterpret_cast<const uint4*>(gb)[1];
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c0 + j;
+        const int n = nb + j;
         if (n >= a.N) continue;
         const float acc = __uint_as_float(r[j]);
         const int64_t o = (int64_t)row * a.ldo + n;

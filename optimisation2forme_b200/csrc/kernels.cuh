@@ -403,7 +403,7 @@ __device__ __forceinline__ void cell_gradient_at(int64_t c,
 }
 
 template <typename T, bool kWriteGrad>
-__global__ void __launch_bounds__(kBlock) k_cell_gradient(
+__global__ void __launch_bounds__(kBlock, 3) k_cell_gradient(
     int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
     const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
     const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
@@ -441,7 +441,7 @@ __device__ __forceinline__ void edge_flux_at(int64_t e, int64_t ne, Geom<T> g, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_edge_flux(int64_t ne, Geom<T> g, const int2* __restrict__ ev,
+__global__ void __launch_bounds__(kBlock, 4) k_edge_flux(int64_t ne, Geom<T> g, const int2* __restrict__ ev,
                                                       const uint8_t* __restrict__ ebc,
                                                       const Vec4<T>* __restrict__ eL,
                                                       const Vec4<T>* __restrict__ eR,

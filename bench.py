@@ -299,6 +299,87 @@ def run_o2f(args, rank: int, world: int) -> dict | None:
     return line if rank == 0 else None
 
 
+def batch_candidates(n: int = 16, seed: int = 0):
+    """Seeded candidates of uneven size for the batched path: NACA (m, p, t)
+    in [0, 0.06] x [0.2, 0.6] x [0.08, 0.18], M in [0.5, 0.8], AoA in [0, 4]
+    deg, O-grids of about 25k-150k triangles (first cell 1e-3 chord)."""
+    from optimisation2forme_b200 import SimulationParams
+    from optimisation2forme_b200.meshgen import OGridSpec, naca_ogrid
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        ns = int(rng.integers(100, 250)) * 2
+        nl = int(rng.integers(60, 150))
+        spec = OGridSpec(m=float(rng.uniform(0, 0.06)), p=float(rng.uniform(0.2, 0.6)), t=float(rng.uniform(0.08, 0.18)),
+                         n_surface=ns, n_layers=nl, first_height=1e-3, growth=1.1, seed=seed + i)
+        params = SimulationParams(viscosity=1.8e-5, inflow_velocity=float(rng.uniform(0.5, 0.8)),
+                                  aoa_deg=float(rng.uniform(0, 4)), cfl_number=0.5, final_time=1e30, limiter_k=5.0,
+                                  adjoint_precond="none", dt_mode="thermal", verbosity=0)
+        out.append((spec, naca_ogrid(spec), params))
+    return out
+
+
+def run_batch(args) -> dict:
+    """Candidates advanced by the batched time loop (one grouped launch per
+    phase for all of them) vs the same candidates one context at a time; each
+    evaluation = RK3 steps + a 100-iteration adjoint chunk + dJ/d(m,p,t)."""
+    import torch
+    from optimisation2forme_b200 import Batch, Solver, mesh_desc
+    from optimisation2forme_b200._lib import ShapeParams
+    torch.cuda.set_device(0)
+    rk_steps = args.rk_steps or 2000
+    cands = batch_candidates()
+    ctxs = [Solver(p, desc=mesh_desc(m["node_xy"], m["segments"], m["segment_bc"], m["cell_offsets"],
+                                    m["cell_nodes"])) for _, m, p in cands]
+    cells = [c.n_cells for c in ctxs]
+    shapes = [ShapeParams(sp.pos_x, sp.chord, sp.m, sp.p, sp.t) for sp, _, _ in cands]
+
+    def adjoint_and_gradient():
+        for s, sh in zip(ctxs, shapes):
+            s.solve_adjoint_system(0.1, tol=1e-8, max_iter=100, restart=100, raise_on_failure=False)
+            s.compute_shape_gradient(["m", "p", "t"], sh, beta=0.1)
+
+    def batched(b):
+        for s in ctxs:
+            s.initialize_freestream()
+        b.time_loop(rk_steps)
+        adjoint_and_gradient()
+
+    def sequential():
+        for s in ctxs:
+            s.initialize_freestream()
+            s.time_loop(rk_steps, raise_on_failure=False)
+        adjoint_and_gradient()
+
+    b = Batch(ctxs)
+    tuned = b.tune(reps=5)
+    for s in ctxs:
+        s.initialize_freestream()
+    finite = sum(r["status"] == "OK" for r in b.time_loop(rk_steps))
+    times = {}
+    for name, fn in (("batched", lambda: batched(b)), ("sequential", sequential)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fn()
+        torch.cuda.synchronize()
+        times[name] = (time.perf_counter() - t0) / args.steps
+    b.close()
+    n = len(ctxs)
+    return {"metric": "batched shape-gradient evals/s (uneven candidates)", "value": n / times["batched"],
+            "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * times["batched"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded NACA O-grids)",
+            "config": {"workload": f"batch: {n} candidates, {sum(cells)} triangles ({min(cells)}-{max(cells)} each), "
+                                   f"{rk_steps} SSP-RK3 steps + 100 BiCGSTAB iterations + dJ/d(m,p,t)",
+                       "candidates_finite": finite,
+                       "sequential_evals_per_s": n / times["sequential"],
+                       "batched_over_sequential": times["sequential"] / times["batched"],
+                       "tuned": {k: list(v) for k, v in tuned.items()}}}
+
+
 def reference_times(mesh: dict, reps: int, threads: int) -> dict:
     """Per-call times of the reference's own computeResidual and
     applyJacobianTranspose (oracle/_ref, OpenMP) on the workload mesh."""
@@ -366,7 +447,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="o2f", choices=["o2f", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "mixed", "small"])
+    ap.add_argument("--workload", default="large", choices=["large", "mixed", "small", "batch"])
     ap.add_argument("--rk-steps", type=int, default=None)
     ap.add_argument("--adjoint-tol", type=float, default=1e-8)
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -385,7 +466,10 @@ def main() -> int:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800))
     try:
-        line = run_reference(args, rank, world) if args.impl == "reference" else run_o2f(args, rank, world)
+        if args.workload == "batch":
+            line = run_batch(args) if rank == 0 and args.impl == "o2f" else None
+        else:
+            line = run_reference(args, rank, world) if args.impl == "reference" else run_o2f(args, rank, world)
     finally:
         if use_pg:
             import torch

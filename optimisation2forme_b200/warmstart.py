@@ -2,7 +2,7 @@
 fields predicts, for a new NACA shape and flow, the state and the adjoint
 field per cell; the adjoint prediction seeds BiCGSTAB, which still converges
 to the same true-residual tolerance (the plain solve is the fallback and
-the judge of the network's error).
+the check on the network's error).
 
 The network (4 x 256 SiLU, Fourier features of the cell centre plus
 (m, p, t, Mach, AoA), BF16 weights/activations, FP32 accumulation) is trained

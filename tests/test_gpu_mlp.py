@@ -1,7 +1,7 @@
 """Warm-start network on the tensor cores (tcgen05 GEMMs, BF16 operands, FP32
 accumulation) against the numpy oracle, its training, and the warm start:
 BiCGSTAB started from the predicted adjoint reaches the same true-residual
-tolerance and the same lambda as from zero (the plain solver judges the
+tolerance and the same lambda as from zero (the plain solver checks the
 prediction), and the test reports both iteration counts."""
 from __future__ import annotations
 

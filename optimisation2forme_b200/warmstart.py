@@ -128,6 +128,34 @@ class Normaliser:
         return t
 
 
+@dataclasses.dataclass
+class InputScaler:
+    """Standardisation of the 7 inputs: the shape and flow parameters (order
+    0.01-1) would otherwise be drowned by the coordinates (up to the far
+    field, 20 chords); the Fourier features then act on standardised (x, y)."""
+    mean: np.ndarray
+    std: np.ndarray
+
+    @classmethod
+    def fit(cls, inputs: np.ndarray) -> "InputScaler":
+        x = np.asarray(inputs, dtype=np.float64).reshape(-1, N_IN)
+        s = x.std(axis=0)
+        return cls(x.mean(axis=0), np.where(s > 0, s, 1.0))
+
+    def apply(self, inputs: np.ndarray) -> np.ndarray:
+        return ((np.asarray(inputs, dtype=np.float64).reshape(-1, N_IN) - self.mean) / self.std).astype(np.float32)
+
+
+def select_fields(targets: Sequence[np.ndarray], factor: float = 10.0) -> list[int]:
+    """Indices of the training fields to keep: a field whose largest adjoint
+    magnitude exceeds `factor` times the median of the fields' maxima comes
+    from a near-singular state (a cell at the edge of positivity) and would
+    dominate the fit; it is left out."""
+    peaks = np.array([np.abs(np.asarray(y).reshape(-1, N_OUT)[:, 4:]).max() for y in targets])
+    ref = np.median(peaks)
+    return [i for i, v in enumerate(peaks) if v <= factor * ref]
+
+
 def cell_inputs(solver, m: float, p: float, t: float) -> np.ndarray:
     """[n_cells, 7] network inputs of a context: cell centres (reference
     order) with the shape and the flow (Mach, AoA) of its parameters."""
@@ -161,14 +189,16 @@ def sample(solver, m: float, p: float, t: float, steps: int, beta: float = 0.1, 
 
 
 def adjoint_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t: float,
-                  beta: float = 0.1, residual_scaled: bool = False) -> np.ndarray:
+                  beta: float = 0.1, residual_scaled: bool = False, scaler: InputScaler | None = None) -> np.ndarray:
     """Predicted lambda (reference order, interleaved 4 per cell).  With
     residual_scaled, it is multiplied by the alpha minimising
     ||b - J^T (alpha lambda0)|| (one J^T product), which bounds the initial
     residual by ||b||; J^T weighs the guess's cell-scale error by 1/h, so
     that alpha can vanish for a guess that is close in L2.  Needs the
-    interface states of the current state."""
-    y = norm.from_net(net.predict(cell_inputs(solver, m, p, t)))
+    interface states of the current state.  `scaler`: the input
+    standardisation the network was trained with."""
+    x = cell_inputs(solver, m, p, t)
+    y = norm.from_net(net.predict(scaler.apply(x) if scaler else x))
     lam0 = np.ascontiguousarray((y[:, 4:8] * _size(solver)).reshape(-1))
     if not residual_scaled:
         return lam0
@@ -179,6 +209,8 @@ def adjoint_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t:
     return alpha * lam0
 
 
-def state_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t: float) -> np.ndarray:
-    y = norm.from_net(net.predict(cell_inputs(solver, m, p, t)))
+def state_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t: float,
+                scaler: InputScaler | None = None) -> np.ndarray:
+    x = cell_inputs(solver, m, p, t)
+    y = norm.from_net(net.predict(scaler.apply(x) if scaler else x))
     return np.ascontiguousarray(y[:, 0:4].reshape(-1))

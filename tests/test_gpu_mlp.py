@@ -85,20 +85,20 @@ def test_training_fits_a_smooth_field():
         assert hist[-20:].mean() < 0.05 * hist[:5].mean()
 
 
-def test_warm_start_converges_to_the_plain_adjoint():
+def test_warm_start_cuts_adjoint_iterations():
     """Train on the solver's own (state, adjoint) fields over a family of
-    shapes, then start the adjoint of an unseen shape from the prediction.
-    Measured on these transient adjoint fields (heavy-tailed, concentrated in
-    the first wall cells): the prediction is far from lambda in L2 and the
-    warm start does NOT save iterations (167 from zero, 166-178 warm); the
-    test therefore checks convergence and equality and prints the counts."""
+    shapes, then start the adjoint of an unseen shape from the prediction:
+    BiCGSTAB reaches the same true-residual tolerance and the same lambda in
+    fewer iterations than from zero.  The inputs are standardised, the
+    adjoint target is lambda / sqrt(V), and fields from near-singular states
+    (adjoint peaks 40-150x the family's) are left out of the training set."""
     from optimisation2forme_b200 import SimulationParams, Solver
-    from optimisation2forme_b200.warmstart import Network, Normaliser, adjoint_guess, sample
+    from optimisation2forme_b200.warmstart import (InputScaler, Network, Normaliser, adjoint_guess, sample,
+                                                   select_fields)
     p0 = SimulationParams(viscosity=1.8e-5, inflow_velocity=0.6, aoa_deg=2.0, cfl_number=0.5, final_time=10.0,
                           limiter_k=5.0, verbosity=0)
-    # 200 RK3 steps on these meshes stay finite for every shape below (the
-    # family of m in {0, 0.02, 0.04} x p in {0.3, 0.5} x t in {0.10, 0.14}
-    # without (0.04, 0.5, 0.10), whose state develops a negative-pressure cell)
+    # 200 RK3 steps stay finite for every shape of the family except
+    # (0.04, 0.5, 0.10), whose state develops a negative-pressure cell
     shapes = [(m, p, t) for m in (0.0, 0.02, 0.04) for p in (0.3, 0.5) for t in (0.10, 0.14)
               if (m, p, t) != (0.04, 0.5, 0.10)]
     xs, ys = [], []
@@ -108,10 +108,12 @@ def test_warm_start_converges_to_the_plain_adjoint():
             x, y = sample(s, m, p, t, steps=200)
             xs.append(x)
             ys.append(y)
-    X, Y = np.concatenate(xs), np.concatenate(ys)
-    norm = Normaliser.fit(Y)
+    keep = select_fields(ys)
+    assert 6 <= len(keep) < len(shapes)  # the near-singular fields are dropped
+    X, Y = np.concatenate([xs[i] for i in keep]), np.concatenate([ys[i] for i in keep])
+    scaler, norm = InputScaler.fit(X), Normaliser.fit(Y)
     with Network(max_batch=8192, freq_scale=4.0, seed=1) as net:
-        net.set_data(X, norm.to_net(Y))
+        net.set_data(scaler.apply(X), norm.to_net(Y))
         hist = net.train(2000, batch=4096, lr=1e-3, seed=3)
         held = (0.03, 0.4, 0.12)  # inside the family, not one of its members
         mesh = small_mesh(triangles=True, n_surface=64, n_layers=16, seed=11, m=held[0], p=held[1], t=held[2])
@@ -119,12 +121,12 @@ def test_warm_start_converges_to_the_plain_adjoint():
             s.initialize_freestream()
             s.time_loop(200)
             cold = s.solve_adjoint_system(beta=0.1, tol=1e-10)
-            guess = adjoint_guess(net, norm, s, *held, beta=0.1)
+            guess = adjoint_guess(net, norm, s, *held, beta=0.1, scaler=scaler)
             warm = s.solve_adjoint_system(beta=0.1, tol=1e-10, guess=guess)
             err0 = np.linalg.norm(guess - cold["lambda"]) / np.linalg.norm(cold["lambda"])
-            print(f"\nwarm start: training loss {hist[0]:.3e} -> {hist[-20:].mean():.3e}; guess rel err {err0:.2e}; "
-                  f"iterations {cold['iters']} -> {warm['iters']}")
+            print(f"\nwarm start: kept {len(keep)}/{len(shapes)} fields; training loss {hist[0]:.3e} -> "
+                  f"{hist[-20:].mean():.3e}; guess rel err {err0:.2e}; iterations {cold['iters']} -> {warm['iters']}")
             assert warm["relres"] <= 1e-10 and cold["relres"] <= 1e-10
             assert np.linalg.norm(warm["lambda"] - cold["lambda"]) <= 1e-6 * np.linalg.norm(cold["lambda"])
-            assert np.isfinite(err0)
-            assert warm["iters"] <= 2 * cold["iters"]
+            assert err0 < 0.6
+            assert warm["iters"] < cold["iters"]

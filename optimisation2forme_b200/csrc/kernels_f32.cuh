@@ -26,13 +26,15 @@ __global__ void __launch_bounds__(kBlock) k_widen(int64_t n, const float* __rest
 // Without kRk, R is written widened to FP64.  With kRk, the SSP-RK3 stage
 // (src/simulation.cpp:159-167) updates the FP64 state U (and U_old at the
 // first stage) with the FP32 residual, refreshes the FP32 shadow U32 and
-// writes the block partial sums of R_rho^2 in FP64.
+// writes the block partial sums of R_rho^2 in FP64.  `keep` (may be null)
+// receives the FP64 state the stage started from (the last stage's input is
+// what the FP64 path linearises about after the loop).
 template <bool kRk>
 __global__ void __launch_bounds__(kBlock) k_cell_residual_mixed(
     int64_t nc, const int32_t* __restrict__ slot, Geom<float> g, const Vec4<float>* __restrict__ F,
     const Vec4<float>* __restrict__ etq, const float* __restrict__ etqy, Vec4<float>* __restrict__ U32,
     Vec4<double>* __restrict__ U, Vec4<double>* __restrict__ Uold, Vec4<double>* __restrict__ R, RkStage rk,
-    const int* gate) {
+    Vec4<double>* __restrict__ keep, const int* gate) {
   __shared__ double smem[kBlock / 32];
   if (gated(gate)) return;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -91,6 +93,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_residual_mixed(
       if (rk.norm_part) r2 = (double)a0 * (double)a0;
       const double dt = *rk.dt;
       Vec4<double> u = U[c];
+      if (keep) keep[c] = u;
       Vec4<double> uo;
       if (rk.snapshot) {
         uo = u;

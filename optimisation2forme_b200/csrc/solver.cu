@@ -763,7 +763,7 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
   }
   auto stage = [&](const RkStage* rk) {
     if (mixed)
-      launch_residual_f32(gate, rk);
+      launch_residual_f32(gate, rk, rk == &s3 ? Ukeep_ : nullptr);
     else
       launch_residual(geom_, work_, U_, gate, false, rk);
   };
@@ -811,7 +811,13 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
                         cudaMemcpyDeviceToHost));
   if (steps_done) *steps_done = fin.step;
   if (t_out) *t_out = fin.t;
-  if (mixed && fin.step > 0) f32_publish_interfaces();
+  // Mixed path: the forces, J, the Jacobian blocks and the adjoint
+  // right-hand side linearise about the last stage's input state, as in the
+  // FP64 path; one FP64 residual of that state gives its interface states.
+  if (mixed && fin.step > 0) {
+    launch_residual(geom_, work_, Ukeep_, nullptr, false, nullptr);
+    sync();
+  }
   have_residual_ = fin.step > 0;
   blk_valid_ = false;
   if (fin.stop == 2) throw Error(O2F_ERR_NONFINITE, "non-finite state or residual in the time loop");

@@ -93,7 +93,7 @@ class Solver {
   void ensure_f32();
   void f32_state_sync();
   void f32_publish_interfaces();
-  void launch_residual_f32(const int* gate, const void* rk);
+  void launch_residual_f32(const int* gate, const void* rk, Vec4<double>* keep = nullptr);
   void f32_blocks();
   void to_internal(const double* ref, Vec4<double>* dev);
   void to_reference(const Vec4<double>* dev, double* ref);
@@ -119,6 +119,7 @@ class Solver {
   Geom<float> geom32_{};
   Work<float> work32_{};
   Vec4<float>* U32_ = nullptr;
+  Vec4<double>* Ukeep_ = nullptr;  // mixed path: input state of the last RK3 stage
   float* blk32_ = nullptr;
   double* norm_part_ = nullptr;
   StepState* step_ = nullptr;

@@ -57,6 +57,7 @@ void Solver::ensure_f32() {
     geom32_.vw = arena_.alloc<float>(t.nnz);
     work32_ = alloc_work_f32();
     U32_ = arena_.alloc<Vec4<float>>(t.nc);
+    Ukeep_ = arena_.alloc<Vec4<double>>(t.nc);
     f32_ready_ = true;
   }
   if (f32_geom_valid_) return;
@@ -84,7 +85,7 @@ void Solver::f32_publish_interfaces() {
   O2F_CUDA(cudaGetLastError());
 }
 
-void Solver::launch_residual_f32(const int* gate, const void* rkp) {
+void Solver::launch_residual_f32(const int* gate, const void* rkp, Vec4<double>* keep) {
   const Topo& t = topo_;
   const Geom<float>& g = geom32_;
   const Work<float>& w = work32_;
@@ -99,10 +100,10 @@ void Solver::launch_residual_f32(const int* gate, const void* rkp) {
   if (rkp) {
     const RkStage rk = *static_cast<const RkStage*>(rkp);
     k_cell_residual_mixed<true><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, w.F, w.etq, w.etqy, U32_, U_, Uold_,
-                                                              work_.R, rk, gate);
+                                                              work_.R, rk, keep, gate);
   } else {
     k_cell_residual_mixed<false><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, w.F, w.etq, w.etqy, U32_, U_, Uold_,
-                                                               work_.R, RkStage{}, gate);
+                                                               work_.R, RkStage{}, nullptr, gate);
   }
   launches_ += 5;
   O2F_CUDA(cudaGetLastError());

@@ -19,14 +19,15 @@ pytestmark = pytest.mark.gpu
 # in the comments).
 TOL_RESIDUAL = 1e-3    # ||R32 - R64|| / ||R64|| per conserved variable (5e-5 .. 1.5e-4)
 TOL_STATE = 1e-4       # max |U32 - U64| / max |U64| per variable after 300 RK3 steps (3e-6 .. 2.3e-5)
-TOL_FORCES = 1e-5      # |dC_L|, |dC_D| relative to max(|C_L|, |C_D|) (4e-7)
+TOL_FORCES = 1e-5      # |dC_L|, |dC_D| relative to max(|C_L|, |C_D|) (1.6e-7)
 TOL_LAMBDA_SAME = 1e-4  # lambda about the same FP64 state, FP32 residual + blocks (1.6e-5)
 # dJ/dshape against the FP64 oracle.  The target of the mixed path is 1e-4;
 # it is NOT met on this developed transient: the interface states of the FP32
 # residual feed the linearisation (J, blocks, RHS), and dJ = dJ_direct -
 # lambda.dR/dtheta cancels strongly, so lambda's 1.6e-5 becomes 4.4e-4.
 TOL_DJ_SAME = 1e-3     # about the same FP64 state (4.4e-4)
-TOL_DJ_WORKFLOW = 2e-3  # the whole mixed workflow, FP32 time loop included (5.5e-4)
+TOL_DJ_WORKFLOW = 2e-3  # the whole mixed workflow, FP32 time loop included (6.4e-4): the
+                        # FP32 trajectory's state drift (2.3e-5) dominates, not the linearisation
 
 
 def _params(**kw):

@@ -14,7 +14,7 @@ work and the line reports the relres it reached.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl o2f|reference]
 
-Under torchrun (N > 1) every rank evaluates its own candidate (weak scaling,
+Under torchrun (N > 1) every rank evaluates a replica of the workload (weak scaling,
 no data-path collective); the max over ranks of the device time is reported.
 ``--impl reference`` times the reference's own OpenMP CPU code (oracle/_ref)
 on the same mesh on rank 0 and prints the same line with "impl": "reference".

@@ -289,8 +289,11 @@ void Mlp::load_batch(const float* inputs_dev, const int* index_dev, int n) {
 
 void Mlp::set_data(const float* inputs, const float* targets, int64_t n) {
   if (n <= 0) throw Error(O2F_ERR_ARG, "empty data set");
-  data_in_ = arena_.alloc<float>(n * kIn);
-  data_out_ = arena_.alloc<float>(n * kOut);
+  if (n > data_cap_) {  // device buffers grow only: repeated calls reuse them
+    data_in_ = arena_.alloc<float>(n * kIn);
+    data_out_ = arena_.alloc<float>(n * kOut);
+    data_cap_ = n;
+  }
   n_data_ = n;
   O2F_CUDA(cudaMemcpyAsync(data_in_, inputs, n * kIn * sizeof(float), cudaMemcpyHostToDevice, stream_));
   O2F_CUDA(cudaMemcpyAsync(data_out_, targets, n * kOut * sizeof(float), cudaMemcpyHostToDevice, stream_));
@@ -304,7 +307,11 @@ void Mlp::train(int steps, int batch, float lr, uint64_t seed, float* loss_hist)
   std::mt19937_64 rng(seed);
   std::uniform_int_distribution<int64_t> pick(0, n_data_ - 1);
   std::vector<int> idx(batch);
-  float* losses = arena_.alloc<float>(steps);
+  if (steps > loss_cap_) {
+    loss_buf_ = arena_.alloc<float>(steps);
+    loss_cap_ = steps;
+  }
+  float* losses = loss_buf_;
   O2F_CUDA(cudaMemsetAsync(losses, 0, steps * sizeof(float), stream_));
   int* pinned = nullptr;
   O2F_CUDA(cudaMallocHost(&pinned, sizeof(int) * batch));

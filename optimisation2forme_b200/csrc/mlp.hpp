@@ -49,7 +49,9 @@ class Mlp {
   float* loss_ = nullptr;
   int* err_ = nullptr;
   float *data_in_ = nullptr, *data_out_ = nullptr;
-  int64_t n_data_ = 0;
+  int64_t n_data_ = 0, data_cap_ = 0;
+  float* loss_buf_ = nullptr;
+  int64_t loss_cap_ = 0;
   float* scratch_in_ = nullptr;
   int64_t scratch_cap_ = 0;
   float* grad_targets_ = nullptr;

@@ -344,8 +344,11 @@ int o2f_mlp_gradients(o2f_mlp* net, const float* inputs, const float* targets, i
 int o2f_mlp_get_params(o2f_mlp* net, float* params, float* freq);
 int o2f_mlp_set_params(o2f_mlp* net, const float* params);
 
-/* No counterpart in the reference.  Residual of the current state (as
- * o2f_residual, interface states left in the context) and its
+/* No counterpart in the reference.  For callers that may not allocate
+ * device memory during a call -- a host time loop calling it every step,
+ * where cudaMalloc would synchronise the device, or a host that owns all
+ * device memory through its own pool or budget.  Residual of the current
+ * state (as o2f_residual, interface states left in the context) and its
  * ||R_rho||_2 written to *norm_out, with NO device allocation on the call:
  * the norm reduction's scratch is a static device array of 33,280 bytes.
  * Limit: meshes of at most 16,777,216 cells (O2F_ERR_ARG beyond).  Calls

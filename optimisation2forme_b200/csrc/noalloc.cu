@@ -1,6 +1,12 @@
 // o2f_residual_norm_noalloc: the residual of the current state and
 // ||R_rho||_2, with no device allocation on the call path.
 //
+// Who needs it: a host that drives the residual every step of its own
+// time loop cannot afford cudaMalloc there (it synchronises the whole
+// device and can stall on the allocator), and a host that hands this
+// library a fixed device-memory budget, or owns all device memory through
+// its own pool, cannot let a call allocate at all.
+//
 // This is a variant of the time loop's norm reduction (k_cell_residual's
 // per-block partial sums of R_rho^2, folded by k_step_norm), whose partial
 // sums live in context memory.  Here the reduction's scratch -- a completion

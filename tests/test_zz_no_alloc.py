@@ -1,5 +1,6 @@
 """o2f_residual_norm_noalloc (scratch in a static device array, no device
-allocation on the call) against the existing entry point o2f_residual.
+allocation on the call, for hosts that may not allocate during a call)
+against the existing entry point o2f_residual.
 
 The file name sorts last, so in a full run the no-alloc call comes after
 every other GPU test; it also passes alone."""

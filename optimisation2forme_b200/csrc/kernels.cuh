@@ -5,7 +5,9 @@
 // reference expression it restates (cited per kernel).  The FP64
 // instantiation is compiled with -fmad=false, so no multiply-add is fused and
 // each operation rounds exactly as the reference's does on x86-64; sqrt and
-// division are IEEE round-to-nearest on both sides.  Summations follow the
+// division are IEEE round-to-nearest on both sides (quotients that share a
+// divisor come from one reciprocal through qdiv, which returns the same bits
+// as the division; qdiv.h).  Summations follow the
 // reference's Cell::edgeIDs / Vertex::cellIDs order, which the host build
 // reproduces (mesh_host.cpp).  The FP64 residual is therefore bit-identical to
 // the reference for the same mesh and state.
@@ -15,6 +17,7 @@
 #include <cstdint>
 
 #include "device_types.hpp"
+#include "qdiv.h"
 
 namespace o2f {
 
@@ -273,8 +276,13 @@ __global__ void __launch_bounds__(kBlock) k_vertex_visc(int64_t nv, const int32_
 // gradient (src/advection.cpp:136-188), neighbour min/max, limiter and
 // interface states (:236-321), and the cell viscous stress and heat flux from
 // the unlimited gradients (src/diffusion.cpp:223-241).
-template <typename T, bool kWriteGrad>
-__device__ __forceinline__ void cell_gradient_at(int64_t c, 
+//
+// kPlain = false divides the Green-Gauss terms by the volume through one
+// reciprocal (qdiv_flag) and returns false, having written nothing, if any
+// quotient left qdiv's range; cell_gradient_at then redoes the cell with
+// kPlain = true (IEEE divisions), out of line.
+template <typename T, bool kWriteGrad, bool kPlain>
+__device__ __forceinline__ bool cell_gradient_body(int64_t c,
     int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
     const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
     const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
@@ -303,6 +311,13 @@ __device__ __forceinline__ void cell_gradient_at(int64_t c,
     }
   }
 
+  // the eight Green-Gauss terms of every edge divide by the cell volume
+  const T ycv = recip_for_div(cv);
+  bool ok = true;
+  auto over_v = [&](T a) -> T {
+    if constexpr (kPlain) return a / cv;
+    else return qdiv_flag(a, cv, ycv, ok);
+  };
   T gx0 = (T)0.0, gx1 = (T)0.0, gx2 = (T)0.0, gx3 = (T)0.0;
   T gy0 = (T)0.0, gy1 = (T)0.0, gy2 = (T)0.0, gy3 = (T)0.0;
   T mn0 = u.a, mn1 = u.b, mn2 = u.c, mn3 = u.d;
@@ -329,14 +344,14 @@ __device__ __forceinline__ void cell_gradient_at(int64_t c,
       enx = -enx;
       eny = -eny;
     }
-    gx0 += er * el * enx / cv;
-    gx1 += eru * el * enx / cv;
-    gx2 += erv * el * enx / cv;
-    gx3 += eE * el * enx / cv;
-    gy0 += er * el * eny / cv;
-    gy1 += eru * el * eny / cv;
-    gy2 += erv * el * eny / cv;
-    gy3 += eE * el * eny / cv;
+    gx0 += over_v(er * el * enx);
+    gx1 += over_v(eru * el * enx);
+    gx2 += over_v(erv * el * enx);
+    gx3 += over_v(eE * el * enx);
+    gy0 += over_v(er * el * eny);
+    gy1 += over_v(eru * el * eny);
+    gy2 += over_v(erv * el * eny);
+    gy3 += over_v(eE * el * eny);
     if (o >= 0) {
       if (un.a < mn0) mn0 = un.a;
       if (un.a > mx0) mx0 = un.a;
@@ -348,6 +363,8 @@ __device__ __forceinline__ void cell_gradient_at(int64_t c,
       if (un.d > mx3) mx3 = un.d;
     }
   }
+
+  if (!kPlain && !ok) return false;
 
   const int kind = ph.limiter;
   T al0 = (T)1.0, al1 = (T)1.0, al2 = (T)1.0, al3 = (T)1.0;
@@ -382,12 +399,13 @@ __device__ __forceinline__ void cell_gradient_at(int64_t c,
 
   // Viscous stress and heat flux at the cell (src/diffusion.cpp:227-240).
   const T mu = (T)ph.mu, gamma = (T)ph.gamma, kappa = (T)ph.kappa;
-  const T uu = u.b / u.a;
-  const T vv = u.c / u.a;
-  const T u_x = (gx1 - uu * gx0) / u.a;
-  const T v_y = (gy2 - vv * gy0) / u.a;
-  const T u_y = (gy1 - uu * gy0) / u.a;
-  const T v_x = (gx2 - vv * gx0) / u.a;
+  const T yrho = recip_for_div(u.a);
+  const T uu = qdiv(u.b, u.a, yrho);
+  const T vv = qdiv(u.c, u.a, yrho);
+  const T u_x = qdiv(gx1 - uu * gx0, u.a, yrho);
+  const T v_y = qdiv(gy2 - vv * gy0, u.a, yrho);
+  const T u_y = qdiv(gy1 - uu * gy0, u.a, yrho);
+  const T v_x = qdiv(gx2 - vv * gx0, u.a, yrho);
   const T two_thirds = (T)(2.0 / 3.0);
   const T tau_xx = (T)2 * mu * u_x - two_thirds * mu * (u_x + v_y);
   const T tau_yy = (T)2 * mu * v_y - two_thirds * mu * (u_x + v_y);
@@ -400,6 +418,26 @@ __device__ __forceinline__ void cell_gradient_at(int64_t c,
     grad[2 * c] = v4<T>(gx0, gx1, gx2, gx3);
     grad[2 * c + 1] = v4<T>(gy0, gy1, gy2, gy3);
   }
+  return true;
+}
+
+template <typename T, bool kWriteGrad>
+__device__ __noinline__ void cell_gradient_plain(int64_t c,
+    int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
+    const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
+    const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad) {
+  cell_gradient_body<T, kWriteGrad, true>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad);
+}
+
+template <typename T, bool kWriteGrad>
+__device__ __forceinline__ void cell_gradient_at(int64_t c,
+    int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
+    const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
+    const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad) {
+  if (!cell_gradient_body<T, kWriteGrad, false>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad))
+    cell_gradient_plain<T, kWriteGrad>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad);
 }
 
 template <typename T, bool kWriteGrad>
@@ -508,6 +546,7 @@ __device__ __forceinline__ double cell_residual_at(int64_t c, int64_t nc, const 
     a3 += sign * f.d * L;
   }
   const T invV = (T)1.0 / cv;
+  const T ycv = recip_for_div(cv, invV);
   a0 *= -invV;
   a1 *= -invV;
   a2 *= -invV;
@@ -529,9 +568,10 @@ __device__ __forceinline__ double cell_residual_at(int64_t c, int64_t nc, const 
     }
     const Vec4<T> t = etq[e];
     const T qy = etqy[e];
-    a1 += t.a * el * enx / cv + t.c * el * eny / cv;
-    a2 += t.c * el * enx / cv + t.b * el * eny / cv;
-    a3 += (uu * t.a + vv * t.c - t.d) * el * enx / cv + (uu * t.c + vv * t.b - qy) * el * eny / cv;
+    a1 += qdiv(t.a * el * enx, cv, ycv) + qdiv(t.c * el * eny, cv, ycv);
+    a2 += qdiv(t.c * el * enx, cv, ycv) + qdiv(t.b * el * eny, cv, ycv);
+    a3 += qdiv((uu * t.a + vv * t.c - t.d) * el * enx, cv, ycv) +
+          qdiv((uu * t.c + vv * t.b - qy) * el * eny, cv, ycv);
   }
   R[c] = v4<T>(a0, a1, a2, a3);
   if (kRk) {

@@ -46,7 +46,8 @@ typedef enum o2f_status {
   O2F_ERR_NONFINITE = -5,  /* NaN/Inf in a state, residual or Krylov scalar   */
   O2F_ERR_NOT_CONVERGED = -6, /* iteration cap reached before tolerance      */
   O2F_ERR_BREAKDOWN = -7,  /* BiCGSTAB breakdown (rho or omega ~ 0)          */
-  O2F_ERR_STATE = -8       /* call order violated (e.g. adjoint before a residual) */
+  O2F_ERR_STATE = -8,      /* call order violated (e.g. adjoint before a residual) */
+  O2F_ERR_INTERNAL = -9    /* host out of memory or an unexpected internal error */
 } o2f_status;
 
 /* Boundary codes, identical to the reference's char codes

@@ -20,6 +20,7 @@ STATUS = {
     -6: "O2F_ERR_NOT_CONVERGED",
     -7: "O2F_ERR_BREAKDOWN",
     -8: "O2F_ERR_STATE",
+    -9: "O2F_ERR_INTERNAL",
 }
 
 PREC_F64 = 0

@@ -52,13 +52,13 @@ int guarded(F&& f) {
     return O2F_ERR_ARG;
   } catch (const std::bad_alloc&) {
     g_last_error = "host out of memory";
-    return O2F_ERR_ARG;
+    return O2F_ERR_INTERNAL;
   } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return O2F_ERR_MESH;
+    g_last_error = std::string("internal error: ") + e.what();
+    return O2F_ERR_INTERNAL;
   } catch (...) {
-    g_last_error = "unknown error";
-    return O2F_ERR_ARG;
+    g_last_error = "unknown internal error";
+    return O2F_ERR_INTERNAL;
   }
 }
 

@@ -154,6 +154,16 @@ int o2f_host_mesh_from_msh(const char* path, o2f_host_mesh** out);
 int o2f_host_mesh_export(const o2f_host_mesh* mesh, const char* which, void* out, int64_t* count);
 int o2f_host_mesh_destroy(o2f_host_mesh* mesh);
 
+/* No counterpart in the reference.  New vertex coordinates for a host mesh
+ * of unchanged topology, node_xy[2*n_nodes] in the description's node order:
+ * volumes, centres, edge normals and centres, the atan2 cell order of the
+ * vertices (Mesh::Mesh, src/mesh.cpp:140-248) and the interpolation weights
+ * are recomputed with the arithmetic of o2f_host_mesh_create, so every
+ * exported array equals that of a mesh created from these coordinates.
+ * O2F_ERR_ARG for non-finite coordinates; O2F_ERR_MESH, mesh unchanged, when
+ * a cell would collapse or change orientation. */
+int o2f_host_mesh_set_coords(o2f_host_mesh* mesh, const double* node_xy);
+
 /* Build a context: replaces navier_stokes::Mesh::Mesh(params)
  * (src/mesh.cpp:7-283; include/mesh.hpp:116) followed by the solver set-up.
  * `stream` is a cudaStream_t (NULL: the context creates its own). */
@@ -357,6 +367,24 @@ int o2f_mlp_set_params(o2f_mlp* net, const float* params);
  * The first call on a device looks up the scratch address
  * (cudaGetSymbolAddress); make it before any stream capture. */
 int o2f_residual_norm_noalloc(o2f_ctx* ctx, double* norm_out);
+
+/* No counterpart in the reference, whose outer loop (mesh_opti/run_opti.sh)
+ * re-meshes each new shape with Gmsh and restarts the solver.  New vertex
+ * coordinates for the context's mesh, same topology (node_xy as for
+ * o2f_host_mesh_set_coords): the device geometry is rebuilt exactly as
+ * o2f_create would build it from these coordinates, the flow state is kept,
+ * and a residual must be evaluated again before o2f_forces or the adjoint
+ * (O2F_ERR_STATE otherwise).  Errors as o2f_host_mesh_set_coords. */
+int o2f_set_vertex_coords(o2f_ctx* ctx, const double* node_xy);
+
+/* No counterpart in the reference.  Moves the context's mesh from the NACA
+ * shape `from` to the shape `to` (m, p, t change; pos_x and c must be equal):
+ * wall vertices by the formula of applyShapePerturbationNACA12
+ * (src/shape_optimization.cpp:828-890; wall vertices at xr >= 0.9 stay),
+ * interior vertices by inverse distance weighting of the boundary
+ * displacements, weights |r|^-power with power in [1, 8], far-field, inlet
+ * and outlet vertices fixed; then as o2f_set_vertex_coords. */
+int o2f_deform_shape(o2f_ctx* ctx, const o2f_shape_params* from, const o2f_shape_params* to, int power);
 
 #ifdef __cplusplus
 }

@@ -158,6 +158,20 @@ int o2f_host_mesh_destroy(o2f_host_mesh* mesh) {
   return guarded([&] { delete mesh; });
 }
 
+int o2f_host_mesh_set_coords(o2f_host_mesh* mesh, const double* node_xy) {
+  return guarded([&] {
+    need(mesh, "mesh");
+    need(node_xy, "node_xy");
+    try {
+      o2f::set_coordinates(mesh->mesh, node_xy);
+    } catch (const std::invalid_argument&) {
+      throw;
+    } catch (const std::runtime_error& e) {
+      throw o2f::Error(O2F_ERR_MESH, e.what());
+    }
+  });
+}
+
 int o2f_create(const o2f_mesh_desc* mesh, const o2f_params* params, void* stream, o2f_ctx** out) {
   return guarded([&] {
     need(mesh, "mesh");
@@ -453,6 +467,21 @@ int o2f_residual_norm_noalloc(o2f_ctx* ctx, double* norm_out) {
   return guarded([&] {
     need(norm_out, "norm_out");
     S(ctx).residual_norm_noalloc(norm_out);
+  });
+}
+
+int o2f_set_vertex_coords(o2f_ctx* ctx, const double* node_xy) {
+  return guarded([&] {
+    need(node_xy, "node_xy");
+    S(ctx).set_vertex_coords(node_xy);
+  });
+}
+
+int o2f_deform_shape(o2f_ctx* ctx, const o2f_shape_params* from, const o2f_shape_params* to, int power) {
+  return guarded([&] {
+    need(from, "from");
+    need(to, "to");
+    S(ctx).deform_shape(*from, *to, power);
   });
 }
 

@@ -33,6 +33,64 @@ struct MeshError : std::runtime_error {
 
 inline double clamp1(double v) { return (v < -1.0) ? -1.0 : (1.0 < v) ? 1.0 : v; }
 
+// Volume and centre of cell c from its vertices (src/mesh.cpp:140-171).
+void cell_geometry(HostMesh& m, int64_t c) {
+  const int64_t o0 = m.cell_voff[c], nn = m.cell_voff[c + 1] - o0;
+  const int64_t* n = &m.cell_verts[o0];
+  const double x0 = m.vx[n[0]], y0 = m.vy[n[0]], x1 = m.vx[n[1]], y1 = m.vy[n[1]], x2 = m.vx[n[2]],
+               y2 = m.vy[n[2]];
+  if (nn == 3) {
+    double ax = x1 - x0, ay = y1 - y0, bx = x2 - x0, by = y2 - y0;
+    m.cvol[c] = std::abs(0.5 * (ax * by - bx * ay));
+    m.ccx[c] = 1.0 / 3.0 * (x0 + x1 + x2);
+    m.ccy[c] = 1.0 / 3.0 * (y0 + y1 + y2);
+  } else {
+    const double x3 = m.vx[n[3]], y3 = m.vy[n[3]];
+    double ax = x1 - x0, ay = y1 - y0, bx = x2 - x0, by = y2 - y0;
+    double cx = x1 - x2, cy = y1 - y2, ex = x3 - x2, ey = y3 - y2;
+    m.cvol[c] = 0.5 * (std::abs(ax * by - bx * ay) + std::abs(cx * ey - ex * cy));
+    m.ccx[c] = 0.25 * (x0 + x1 + x2 + x3);
+    m.ccy[c] = 0.25 * (y0 + y1 + y2 + y3);
+  }
+}
+
+// Length, unit normal toward the left cell and centre of edge e
+// (src/mesh.cpp:196-222); needs the left cell's centre.
+void edge_geometry(HostMesh& m, int64_t e) {
+  const int64_t a = m.e_v0[e], b = m.e_v1[e], cl = m.e_cl[e];
+  double tx = m.vx[a] - m.vx[b], ty = m.vy[a] - m.vy[b], tz = 0.0;
+  double len = std::sqrt(tx * tx + ty * ty + tz * tz);
+  double nx = ty / len, ny = -tx / len;
+  double ex = 0.5 * (m.vx[a] + m.vx[b]), ey = 0.5 * (m.vy[a] + m.vy[b]);
+  double dx = m.ccx[cl] - ex, dy = m.ccy[cl] - ey;
+  if (dx * nx + dy * ny < 0) {
+    nx = -nx;
+    ny = -ny;
+  }
+  m.elen[e] = len;
+  m.enx[e] = nx;
+  m.eny[e] = ny;
+  m.ecx[e] = ex;
+  m.ecy[e] = ey;
+}
+
+// Vertex::cellIDsOrdered: the cells of every vertex sorted by the angle of
+// their centre about the vertex (src/mesh.cpp:238-247).
+void vertex_cell_order(HostMesh& m) {
+  m.vert_cells_ord.clear();
+  m.vert_cells_ord.reserve(m.vert_cells.size());
+  std::vector<std::pair<double, int64_t>> tmp;
+  for (int64_t v = 0; v < m.nv; ++v) {
+    tmp.clear();
+    for (int64_t k = m.vert_coff[v]; k < m.vert_coff[v + 1]; ++k) {
+      const int64_t c = m.vert_cells[k];
+      tmp.emplace_back(std::atan2(m.ccy[c] - m.vy[v], m.ccx[c] - m.vx[v]), c);
+    }
+    std::sort(tmp.begin(), tmp.end(), [](auto& a, auto& b) { return a.first < b.first; });
+    for (auto& pr : tmp) m.vert_cells_ord.push_back(pr.second);
+  }
+}
+
 }  // namespace
 
 HostMesh build_mesh(const o2f_mesh_desc& d) {
@@ -91,21 +149,7 @@ HostMesh build_mesh(const o2f_mesh_desc& d) {
       m.cell_verts.push_back(n[k]);
     }
     m.cell_voff[c + 1] = (int64_t)m.cell_verts.size();
-    const double x0 = m.vx[n[0]], y0 = m.vy[n[0]], x1 = m.vx[n[1]], y1 = m.vy[n[1]], x2 = m.vx[n[2]],
-                 y2 = m.vy[n[2]];
-    if (nn == 3) {
-      double ax = x1 - x0, ay = y1 - y0, bx = x2 - x0, by = y2 - y0;
-      m.cvol[c] = std::abs(0.5 * (ax * by - bx * ay));
-      m.ccx[c] = 1.0 / 3.0 * (x0 + x1 + x2);
-      m.ccy[c] = 1.0 / 3.0 * (y0 + y1 + y2);
-    } else {
-      const double x3 = m.vx[n[3]], y3 = m.vy[n[3]];
-      double ax = x1 - x0, ay = y1 - y0, bx = x2 - x0, by = y2 - y0;
-      double cx = x1 - x2, cy = y1 - y2, ex = x3 - x2, ey = y3 - y2;
-      m.cvol[c] = 0.5 * (std::abs(ax * by - bx * ay) + std::abs(cx * ey - ex * cy));
-      m.ccx[c] = 0.25 * (x0 + x1 + x2 + x3);
-      m.ccy[c] = 0.25 * (y0 + y1 + y2 + y3);
-    }
+    cell_geometry(m, c);
     for (int64_t k = 0; k < nn; ++k) vcells[n[k]].insert((std::size_t)c);
     for (int64_t k = 0; k < nn; ++k) record_edge(n[k], n[(k + 1) % nn], c);
   }
@@ -133,20 +177,7 @@ HostMesh build_mesh(const o2f_mesh_desc& d) {
     if (itbc != bc.end()) m.ebc[e] = itbc->second;
     if (cr == -1 && m.ebc[e] == 0) throw MeshError("boundary edge without a boundary condition");
     if (cr != -1 && m.ebc[e] != 0) throw MeshError("interior edge carries a boundary condition");
-    double tx = m.vx[a] - m.vx[b], ty = m.vy[a] - m.vy[b], tz = 0.0;
-    double len = std::sqrt(tx * tx + ty * ty + tz * tz);
-    double nx = ty / len, ny = -tx / len;
-    double ex = 0.5 * (m.vx[a] + m.vx[b]), ey = 0.5 * (m.vy[a] + m.vy[b]);
-    double dx = m.ccx[cl] - ex, dy = m.ccy[cl] - ey;
-    if (dx * nx + dy * ny < 0) {
-      nx = -nx;
-      ny = -ny;
-    }
-    m.elen[e] = len;
-    m.enx[e] = nx;
-    m.eny[e] = ny;
-    m.ecx[e] = ex;
-    m.ecy[e] = ey;
+    edge_geometry(m, e);
     cedges[cl].insert((std::size_t)e);
     if (cr != -1) {
       cedges[cr].insert((std::size_t)e);
@@ -168,25 +199,59 @@ HostMesh build_mesh(const o2f_mesh_desc& d) {
   }
   // Vertex cell lists and the atan2 order (src/mesh.cpp:231-248).
   m.vert_coff.assign(m.nv + 1, 0);
-  std::vector<std::pair<double, std::size_t>> tmp;
   for (int64_t v = 0; v < m.nv; ++v) {
-    tmp.clear();
-    for (auto c : vcells[v]) {
-      m.vert_cells.push_back((int64_t)c);
-      tmp.emplace_back(std::atan2(m.ccy[c] - m.vy[v], m.ccx[c] - m.vx[v]), c);
-    }
-    std::sort(tmp.begin(), tmp.end(), [](auto& a, auto& b) { return a.first < b.first; });
-    for (auto& pr : tmp) m.vert_cells_ord.push_back((int64_t)pr.second);
+    for (auto c : vcells[v]) m.vert_cells.push_back((int64_t)c);
     m.vert_coff[v + 1] = (int64_t)m.vert_cells.size();
     m.max_valence = std::max<int64_t>(m.max_valence, (int64_t)vcells[v].size());
     std::unordered_set<std::size_t>().swap(vcells[v]);
   }
+  vertex_cell_order(m);
   for (int64_t c = 0; c < m.nc; ++c) {
     int64_t n = m.cell_eoff[c + 1] - m.cell_eoff[c];
     if (n != m.cell_voff[c + 1] - m.cell_voff[c]) throw MeshError("cell with a repeated vertex");
   }
   compute_vertex_weights(m);
   return m;
+}
+
+namespace {
+
+// Twice the signed area of cell c (shoelace over its vertices in file order).
+double signed_area2(const HostMesh& m, int64_t c) {
+  const int64_t o0 = m.cell_voff[c], nn = m.cell_voff[c + 1] - o0;
+  double a = 0.0;
+  for (int64_t k = 0; k < nn; ++k) {
+    const int64_t i = m.cell_verts[o0 + k], j = m.cell_verts[o0 + (k + 1) % nn];
+    a += m.vx[i] * m.vy[j] - m.vx[j] * m.vy[i];
+  }
+  return a;
+}
+
+}  // namespace
+
+void set_coordinates(HostMesh& m, const double* xy) {
+  if (!xy) throw std::invalid_argument("null coordinates");
+  for (int64_t i = 0; i < 2 * m.nv; ++i)
+    if (!std::isfinite(xy[i])) throw std::invalid_argument("non-finite vertex coordinate");
+  std::vector<double> ox = m.vx, oy = m.vy;
+  std::vector<int8_t> side(m.nc);
+  for (int64_t c = 0; c < m.nc; ++c) side[c] = signed_area2(m, c) > 0.0 ? 1 : -1;
+  for (int64_t v = 0; v < m.nv; ++v) {
+    m.vx[v] = xy[2 * v];
+    m.vy[v] = xy[2 * v + 1];
+  }
+  for (int64_t c = 0; c < m.nc; ++c) {
+    const double a = signed_area2(m, c);
+    if (a == 0.0 || (a > 0.0 ? 1 : -1) != side[c]) {
+      m.vx.swap(ox);
+      m.vy.swap(oy);
+      throw MeshError("the new coordinates fold or collapse cell " + std::to_string(c));
+    }
+  }
+  for (int64_t c = 0; c < m.nc; ++c) cell_geometry(m, c);
+  for (int64_t e = 0; e < m.ne; ++e) edge_geometry(m, e);
+  vertex_cell_order(m);
+  compute_vertex_weights(m);
 }
 
 void compute_vertex_weights(HostMesh& m) {

@@ -35,6 +35,16 @@ struct HostMesh {
 };
 
 HostMesh build_mesh(const o2f_mesh_desc& desc);
+
+// New vertex coordinates (xy[2*v], xy[2*v+1] in file order) for a built mesh
+// of the same topology: every geometric quantity (cell volumes and centres,
+// edge lengths, normals and centres, the atan2 cell order of the vertices,
+// interpolation weights) is recomputed with the arithmetic of build_mesh, so
+// the result equals build_mesh of a description with these coordinates.
+// Throws std::invalid_argument for non-finite coordinates and a
+// std::runtime_error, leaving the mesh unchanged, when a cell would collapse
+// or change orientation.
+void set_coordinates(HostMesh& m, const double* xy);
 // Reads an ASCII MSH 2.2 file the way the reference's Gmsh import sees it and
 // returns the equivalent description (the vectors own the storage).
 struct MshData {

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <numeric>
 
+#include "deform.cuh"
 #include "ilu.cuh"
 #include "kernels_adjoint.cuh"
 
@@ -164,7 +165,6 @@ void Solver::upload_mesh() {
   // Cells.
   std::vector<int32_t> slot(4 * nc, -1), jslot(4 * nc, -1), cverts(4 * nc, -1);
   std::vector<uint8_t> ctype(nc);
-  std::vector<Vec4<double>> cgeom(nc);
   for (int64_t c = 0; c < nc; ++c) {
     const int64_t co = cperm_[c];
     const int64_t o0 = m.cell_eoff[co], o1 = m.cell_eoff[co + 1];
@@ -183,38 +183,24 @@ void Solver::upload_mesh() {
     const int64_t v0 = m.cell_voff[co], v1 = m.cell_voff[co + 1];
     ctype[c] = (uint8_t)(v1 - v0);
     for (int64_t k = 0; k < v1 - v0; ++k) cverts[4 * c + k] = (int32_t)vinv_[m.cell_verts[v0 + k]];
-    cgeom[c] = Vec4<double>{m.ccx[co], m.ccy[co], m.cvol[co], 0.0};
   }
   // Edges.
   std::vector<int2> ev(ne), ec(ne);
   std::vector<uint8_t> ebc(ne);
-  std::vector<Vec4<double>> egeom(ne);
-  std::vector<Vec2<double>> ectr(ne);
   for (int64_t e = 0; e < ne; ++e) {
     const int64_t eo = eperm_[e];
     ev[e] = make_int2((int)vinv_[m.e_v0[eo]], (int)vinv_[m.e_v1[eo]]);
     ec[e] = make_int2((int)cinv_[m.e_cl[eo]], m.e_cr[eo] >= 0 ? (int)cinv_[m.e_cr[eo]] : -1);
     ebc[e] = m.ebc[eo];
-    egeom[e] = Vec4<double>{m.enx[eo], m.eny[eo], m.elen[eo], 0.0};
-    ectr[e] = Vec2<double>{m.ecx[eo], m.ecy[eo]};
   }
   // Vertices.
-  std::vector<int32_t> voff(nv + 1), vcid(topo_.nnz);
-  std::vector<double> vw(topo_.nnz);
+  std::vector<int32_t> voff(nv + 1);
   std::vector<uint8_t> vbc(nv);
-  std::vector<Vec2<double>> vxy(nv);
   voff[0] = 0;
   for (int64_t v = 0; v < nv; ++v) {
     const int64_t vo = vperm_[v];
-    const int64_t o0 = m.vert_coff[vo], o1 = m.vert_coff[vo + 1];
-    for (int64_t k = o0; k < o1; ++k) {
-      const int64_t j = voff[v] + (k - o0);
-      vcid[j] = (int32_t)cinv_[m.vert_wcells[k]];
-      vw[j] = m.vert_w[k];
-    }
-    voff[v + 1] = voff[v] + (int32_t)(o1 - o0);
+    voff[v + 1] = voff[v] + (int32_t)(m.vert_coff[vo + 1] - m.vert_coff[vo]);
     vbc[v] = m.vbc[vo];
-    vxy[v] = Vec2<double>{m.vx[vo], m.vy[vo]};
   }
   // Wall edges in ascending reference id; cells owning them.
   wall_edges_host_.clear();
@@ -263,8 +249,6 @@ void Solver::upload_mesh() {
   topo_.ec = arena_.alloc<int2>(ne);
   topo_.ebc = arena_.alloc<uint8_t>(ne);
   topo_.voff = arena_.alloc<int32_t>(nv + 1);
-  topo_.vcid = arena_.alloc<int32_t>(vcid.size());
-  topo_.vcid_ord = topo_.vcid;
   topo_.vbc = arena_.alloc<uint8_t>(nv);
   topo_.n_wall = (int64_t)wall_edges_host_.size();
   topo_.wall_edges = arena_.alloc<int32_t>(wall_edges_host_.size());
@@ -288,7 +272,6 @@ void Solver::upload_mesh() {
   h2d(topo_.ec, ec, s);
   h2d(topo_.ebc, ebc, s);
   h2d(topo_.voff, voff, s);
-  h2d(topo_.vcid, vcid, s);
   h2d(topo_.vbc, vbc, s);
   h2d(topo_.wall_edges, wall_edges_host_, s);
   h2d(topo_.wall_cells, wall_cells, s);
@@ -299,16 +282,7 @@ void Solver::upload_mesh() {
   h2d(topo_.pert_cells, pcells, s);
   h2d(topo_.pert_wverts, pwverts, s);
 
-  geom_.cgeom = arena_.alloc<Vec4<double>>(nc);
-  geom_.egeom = arena_.alloc<Vec4<double>>(ne);
-  geom_.ectr = arena_.alloc<Vec2<double>>(ne);
-  geom_.vxy = arena_.alloc<Vec2<double>>(nv);
-  geom_.vw = arena_.alloc<double>(vw.size());
-  h2d(geom_.cgeom, cgeom, s);
-  h2d(geom_.egeom, egeom, s);
-  h2d(geom_.ectr, ectr, s);
-  h2d(geom_.vxy, vxy, s);
-  h2d(geom_.vw, vw, s);
+  upload_geometry();
 
   work_ = alloc_work();
   U_ = arena_.alloc<Vec4<double>>(nc);
@@ -323,6 +297,123 @@ void Solver::upload_mesh() {
   O2F_CUDA(cudaMemsetAsync(ks_, 0, sizeof(KrylovState), s));
   sync();  // host staging vectors go out of scope
   setup_ilu_host(jslot, ec, ebc);
+}
+
+// Geometry of the host mesh in device order: cell centres and volumes, edge
+// normals, lengths and centres, vertex coordinates, and the interpolation
+// weights with their cells (the weights' cell order follows the geometry:
+// Vertex::cellIDsOrdered).  The buffers are allocated on the first call and
+// overwritten by later ones (set_vertex_coords), so captured graphs stay valid.
+void Solver::upload_geometry() {
+  const HostMesh& m = hm_;
+  const int64_t nc = m.nc, ne = m.ne, nv = m.nv;
+  std::vector<Vec4<double>> cgeom(nc);
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t co = cperm_[c];
+    cgeom[c] = Vec4<double>{m.ccx[co], m.ccy[co], m.cvol[co], 0.0};
+  }
+  std::vector<Vec4<double>> egeom(ne);
+  std::vector<Vec2<double>> ectr(ne);
+  for (int64_t e = 0; e < ne; ++e) {
+    const int64_t eo = eperm_[e];
+    egeom[e] = Vec4<double>{m.enx[eo], m.eny[eo], m.elen[eo], 0.0};
+    ectr[e] = Vec2<double>{m.ecx[eo], m.ecy[eo]};
+  }
+  std::vector<int32_t> vcid(topo_.nnz);
+  std::vector<double> vw(topo_.nnz);
+  std::vector<Vec2<double>> vxy(nv);
+  int64_t j = 0;
+  for (int64_t v = 0; v < nv; ++v) {
+    const int64_t vo = vperm_[v];
+    for (int64_t k = m.vert_coff[vo]; k < m.vert_coff[vo + 1]; ++k, ++j) {
+      vcid[j] = (int32_t)cinv_[m.vert_wcells[k]];
+      vw[j] = m.vert_w[k];
+    }
+    vxy[v] = Vec2<double>{m.vx[vo], m.vy[vo]};
+  }
+  if (!geom_.cgeom) {
+    topo_.vcid = arena_.alloc<int32_t>(vcid.size());
+    topo_.vcid_ord = topo_.vcid;
+    geom_.cgeom = arena_.alloc<Vec4<double>>(nc);
+    geom_.egeom = arena_.alloc<Vec4<double>>(ne);
+    geom_.ectr = arena_.alloc<Vec2<double>>(ne);
+    geom_.vxy = arena_.alloc<Vec2<double>>(nv);
+    geom_.vw = arena_.alloc<double>(vw.size());
+  }
+  cudaStream_t s = stream_;
+  h2d(topo_.vcid, vcid, s);
+  h2d(geom_.cgeom, cgeom, s);
+  h2d(geom_.egeom, egeom, s);
+  h2d(geom_.ectr, ectr, s);
+  h2d(geom_.vxy, vxy, s);
+  h2d(geom_.vw, vw, s);
+  sync();  // the staging vectors go out of scope
+}
+
+void Solver::set_vertex_coords(const double* xy) {
+  try {
+    set_coordinates(hm_, xy);
+  } catch (const std::invalid_argument& e) {
+    throw Error(O2F_ERR_ARG, e.what());
+  } catch (const std::runtime_error& e) {
+    throw Error(O2F_ERR_MESH, e.what());
+  }
+  min_h_ = min_cell_h(hm_);
+  upload_geometry();
+  set_params(params_);  // limiter eps from the new volumes; J^T blocks and FP32 geometry invalid
+  have_residual_ = false;
+  have_lambda_ = false;
+}
+
+void Solver::deform_shape(const o2f_shape_params& from, const o2f_shape_params& to, int power) {
+  if (power < 1 || power > 8) throw Error(O2F_ERR_ARG, "IDW power must be in [1, 8]");
+  if (from.pos_x != to.pos_x || from.c != to.c)
+    throw Error(O2F_ERR_ARG, "deform_shape moves m, p, t; pos_x and c must not change");
+  const int64_t nv = topo_.nv;
+  cudaStream_t s = stream_;
+  if (!deform_alloc_) {
+    std::vector<uint8_t> vbc(nv);
+    for (int64_t v = 0; v < nv; ++v) vbc[v] = hm_.vbc[vperm_[v]];
+    std::vector<int32_t> src;
+    for (int64_t v = 0; v < nv; ++v)
+      if (vbc[v] != 0) src.push_back((int32_t)v);
+    if (src.empty()) throw Error(O2F_ERR_MESH, "the mesh has no boundary vertices");
+    n_idw_src_ = (int64_t)src.size();
+    idw_src_ = arena_.alloc<int32_t>(src.size());
+    idw_sxy_ = arena_.alloc<Vec2<double>>(src.size());
+    idw_sd_ = arena_.alloc<Vec2<double>>(src.size());
+    dvxy_ = arena_.alloc<Vec2<double>>(nv);
+    h2d(idw_src_, src, s);
+    sync();
+    deform_alloc_ = true;
+  }
+  // wall vertices to the new shape (the perturbation of the shape gradient)
+  O2F_CUDA(cudaMemcpyAsync(dvxy_, geom_.vxy, nv * sizeof(Vec2<double>), cudaMemcpyDeviceToDevice, s));
+  ShapeArgs a{};
+  a.pos_x = from.pos_x;
+  a.c = from.c;
+  a.m0 = from.m;
+  a.p0 = from.p;
+  a.t0 = from.t;
+  a.m1 = to.m;
+  a.p1 = to.p;
+  a.t1 = to.t;
+  if (topo_.n_pert_verts)
+    k_perturb_vertices<<<grid(topo_.n_pert_verts), kBlock, 0, s>>>(topo_.n_pert_verts, topo_.pert_verts, a, dvxy_);
+  k_idw_sources<<<grid(n_idw_src_), kBlock, 0, s>>>(n_idw_src_, idw_src_, geom_.vxy, dvxy_, idw_sxy_, idw_sd_);
+  k_idw_deform<<<(int)((nv + kIdwTile - 1) / kIdwTile), kIdwTile, 0, s>>>(nv, topo_.vbc, geom_.vxy, n_idw_src_,
+                                                                       idw_sxy_, idw_sd_, power, dvxy_);
+  O2F_CUDA(cudaGetLastError());
+  launches_ += 3;
+  std::vector<Vec2<double>> moved(nv);
+  O2F_CUDA(cudaMemcpyAsync(moved.data(), dvxy_, nv * sizeof(Vec2<double>), cudaMemcpyDeviceToHost, s));
+  sync();
+  std::vector<double> xy(2 * nv);
+  for (int64_t v = 0; v < nv; ++v) {
+    xy[2 * vperm_[v]] = moved[v].a;
+    xy[2 * vperm_[v] + 1] = moved[v].b;
+  }
+  set_vertex_coords(xy.data());
 }
 
 // Reverse Cuthill-McKee order of the cell adjacency graph (BFS from a

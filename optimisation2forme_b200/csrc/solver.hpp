@@ -74,11 +74,18 @@ class Solver {
   void debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which, double* out);
   void profile_kernels(int reps, double* ms_out);
   void residual_norm_noalloc(double* norm_out);  // noalloc.cu
+  // New vertex coordinates (reference order) for the same topology: the
+  // geometry is rebuilt as for a fresh context on those coordinates.
+  void set_vertex_coords(const double* xy_ref);
+  // Wall to the shape `to` by the perturbation formula, interior by inverse
+  // distance weighting of the boundary displacements (deform.cuh).
+  void deform_shape(const o2f_shape_params& from, const o2f_shape_params& to, int power);
   double last_residual_ms() const { return last_residual_ms_; }
   int64_t launches() const { return launches_; }
 
  private:
   void upload_mesh();
+  void upload_geometry();
   void compute_phys();
   void launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<double>* U, const int* gate,
                        bool write_grad, const void* rk);
@@ -152,6 +159,11 @@ class Solver {
   Work<double> pwork_{};
   Vec4<double>* Rp_ = nullptr;
   bool pert_alloc_ = false;
+  // mesh deformation
+  bool deform_alloc_ = false;
+  int64_t n_idw_src_ = 0;
+  int32_t* idw_src_ = nullptr;
+  Vec2<double>*idw_sxy_ = nullptr, *idw_sd_ = nullptr, *dvxy_ = nullptr;
   double last_residual_ms_ = 0.0;
   int64_t launches_ = 0;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;

@@ -6,10 +6,14 @@ Per iteration, as in the reference: march the flow of the current shape from
 the previous iteration's state (run_opti.sh rewrites state_load_path to the
 last saved flow), compute J, the adjoint and dJ/d(m, p), then move m and p by
 fixed steps against the sign of their gradients, clamped
-(run_opti.sh:6-14, 114-131).  The seeded O-grid generator keeps the mesh
-topology when (m, p) change, so the state and the adjoint carry over cell by
-cell; the adjoint of each iteration starts from the previous lambda (a warm
-start that the plain BiCGSTAB then converges from, to the same tolerance).
+(run_opti.sh:6-14, 114-131).  The mesh of the new shape has the topology of
+the first one, so the state and the adjoint carry over cell by cell; the
+adjoint of each iteration starts from the previous lambda (a warm start that
+the plain BiCGSTAB then converges from, to the same tolerance).  The mesh of
+the new shape comes either from the seeded O-grid generator (regenerate: a
+new context per iteration) or from moving the current mesh on the GPU
+(deform: one context for the whole loop, wall by the perturbation formula,
+interior by inverse distance weighting; the state never leaves the device).
 """
 from __future__ import annotations
 
@@ -45,10 +49,17 @@ class SignDescent:
 
 def optimise(spec: OGridSpec, params: SimulationParams, iterations: int, rk_steps: int, beta: float = 50.0,
              rule: SignDescent | None = None, warm_adjoint: bool = True, tol: float = 1e-6,
-             max_iter: int = 100000, stream: int | None = None) -> list[dict]:
+             max_iter: int = 100000, stream: int | None = None, mesh_update: str = "regenerate",
+             idw_power: int = 4) -> list[dict]:
     """Run `iterations` steps of the loop from spec's (m, p); returns one
     record per iteration: m, p, J, C_L, C_D, dJ/dm, dJ/dp, adjoint
-    iterations and relres, time-loop steps."""
+    iterations and relres, time-loop steps.  mesh_update: "regenerate" or
+    "deform" (see the module docstring)."""
+    if mesh_update == "deform":
+        return _optimise_deform(spec, params, iterations, rk_steps, beta, rule or SignDescent(), warm_adjoint, tol,
+                                max_iter, stream, idw_power)
+    if mesh_update != "regenerate":
+        raise ValueError("mesh_update must be 'regenerate' or 'deform'")
     rule = rule or SignDescent()
     m, p = spec.m, spec.p
     U = lam = None
@@ -77,6 +88,36 @@ def optimise(spec: OGridSpec, params: SimulationParams, iterations: int, rk_step
                         "dJ_dp": float(g[1]), "adjoint_iters": adj["iters"], "adjoint_relres": adj["relres"],
                         "adjoint_status": adj["status"], "steps": run["steps"]})
         m, p = rule.step(m, p, float(g[0]), float(g[1]))
+    return history
+
+
+def _optimise_deform(spec, params, iterations, rk_steps, beta, rule, warm_adjoint, tol, max_iter, stream,
+                     idw_power) -> list[dict]:
+    m, p = spec.m, spec.p
+    mesh = naca_ogrid(spec)
+    history = []
+    lam = None
+
+    def shape(m_, p_):
+        return Solver.shape_params(["pos_x", "c", "m", "p", "t"], [spec.pos_x, spec.chord, m_, p_, spec.t])
+
+    with Solver(params, desc=mesh_desc(mesh["node_xy"], mesh["segments"], mesh["segment_bc"],
+                                       mesh["cell_offsets"], mesh["cell_nodes"]), stream=stream) as s:
+        s.initialize_freestream()
+        for k in range(iterations):
+            run = s.time_loop(rk_steps)
+            C_L, C_D, J = s.lift_drag(beta)
+            adj = s.solve_adjoint_system(beta, tol=tol, max_iter=max_iter, raise_on_failure=False,
+                                         guess=lam if (warm_adjoint and lam is not None) else None)
+            g = s.compute_shape_gradient(["m", "p"], shape(m, p), beta=beta, lam=adj["lambda"])
+            lam = adj["lambda"] if adj["status"] == "OK" else None
+            history.append({"iteration": k, "m": m, "p": p, "J": J, "C_L": C_L, "C_D": C_D, "dJ_dm": float(g[0]),
+                            "dJ_dp": float(g[1]), "adjoint_iters": adj["iters"], "adjoint_relres": adj["relres"],
+                            "adjoint_status": adj["status"], "steps": run["steps"]})
+            m_new, p_new = rule.step(m, p, float(g[0]), float(g[1]))
+            if k + 1 < iterations:
+                s.deform_shape(shape(m, p), shape(m_new, p_new), power=idw_power)
+            m, p = m_new, p_new
     return history
 
 

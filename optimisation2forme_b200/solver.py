@@ -234,6 +234,13 @@ class HostMesh:
         check(lib().o2f_host_mesh_export(self._h, name.encode(), out.ctypes.data_as(C.c_void_p), C.byref(n)))
         return out
 
+    def set_coords(self, node_xy: np.ndarray) -> None:
+        """New vertex coordinates, same topology (o2f_host_mesh_set_coords)."""
+        xy = np.ascontiguousarray(node_xy, dtype=np.float64).reshape(-1)
+        if xy.size != self.array("vert_xy").size:
+            raise ValueError("node_xy must hold 2 values per vertex")
+        check(lib().o2f_host_mesh_set_coords(self._h, _ptr(xy)))
+
 
 class Solver:
     """A device-resident mesh + state: the counterpart of the reference's
@@ -289,6 +296,20 @@ class Solver:
         if U.size != 4 * self.n_cells:
             raise ValueError("state must hold 4 values per cell")
         check(lib().o2f_state_set(self._h, _ptr(U)))
+
+    def set_vertex_coords(self, node_xy: np.ndarray) -> None:
+        """New vertex coordinates for the same topology (o2f_set_vertex_coords):
+        geometry as a fresh context on them would have, state kept."""
+        xy = np.ascontiguousarray(node_xy, dtype=np.float64).reshape(-1)
+        if xy.size != 2 * self.n_vertices:
+            raise ValueError("node_xy must hold 2 values per vertex")
+        check(lib().o2f_set_vertex_coords(self._h, _ptr(xy)))
+
+    def deform_shape(self, frm: _lib.ShapeParams, to: _lib.ShapeParams, power: int = 4) -> None:
+        """Move the mesh from shape `frm` to shape `to` (o2f_deform_shape): wall
+        by the reference's perturbation formula, interior by inverse distance
+        weighting with weights |r|^-power."""
+        check(lib().o2f_deform_shape(self._h, C.byref(frm), C.byref(to), int(power)))
 
     def get_state(self) -> np.ndarray:
         U = np.empty(4 * self.n_cells)

@@ -164,6 +164,19 @@ int o2f_host_mesh_destroy(o2f_host_mesh* mesh);
  * a cell would collapse or change orientation. */
 int o2f_host_mesh_set_coords(o2f_host_mesh* mesh, const double* node_xy);
 
+/* Binary state checkpoint, alongside the reference's text state file
+ * (saveCellStates / loadCellStates, src/utils.cpp:29-107), which it does not
+ * replace.  The same values in the same cell order, exactly: a 64-byte header
+ * (magic "O2FSOA1", version, field count, cell count, time, steps, FNV-1a
+ * hash of the payload) and the four conserved fields as contiguous float64
+ * arrays.  U_host: 4 values per cell, interleaved (4i+k), mesh-file cell
+ * order, as o2f_state_set / o2f_state_get.  Host only (no GPU).
+ * o2f_checkpoint_read: O2F_ERR_IO for a missing, foreign, truncated or
+ * corrupted file and for a cell count other than n_cells; time and steps
+ * may be NULL. */
+int o2f_checkpoint_write(const char* path, int64_t n_cells, const double* U_host, double time, int64_t steps);
+int o2f_checkpoint_read(const char* path, int64_t n_cells, double* U_host, double* time, int64_t* steps);
+
 /* Build a context: replaces navier_stokes::Mesh::Mesh(params)
  * (src/mesh.cpp:7-283; include/mesh.hpp:116) followed by the solver set-up.
  * `stream` is a cudaStream_t (NULL: the context creates its own). */

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "batch.hpp"
+#include "checkpoint.hpp"
 #include "mesh_host.hpp"
 #include "mlp.hpp"
 #include "o2f.h"
@@ -169,6 +170,22 @@ int o2f_host_mesh_set_coords(o2f_host_mesh* mesh, const double* node_xy) {
     } catch (const std::runtime_error& e) {
       throw o2f::Error(O2F_ERR_MESH, e.what());
     }
+  });
+}
+
+int o2f_checkpoint_write(const char* path, int64_t n_cells, const double* U_host, double time, int64_t steps) {
+  return guarded([&] {
+    need(path, "path");
+    need(U_host, "U");
+    o2f::checkpoint_write(path, n_cells, U_host, time, steps);
+  });
+}
+
+int o2f_checkpoint_read(const char* path, int64_t n_cells, double* U_host, double* time, int64_t* steps) {
+  return guarded([&] {
+    need(path, "path");
+    need(U_host, "U");
+    o2f::checkpoint_read(path, n_cells, U_host, time, steps);
   });
 }
 

@@ -185,6 +185,26 @@ def _ptr(a: np.ndarray, ct=C.c_double):
     return a.ctypes.data_as(C.POINTER(ct))
 
 
+def save_state_binary(path: str | os.PathLike, U: np.ndarray, time: float = 0.0, steps: int = 0) -> None:
+    """Binary checkpoint of a state (o2f_checkpoint_write): the values of the
+    reference's text state file, bit for bit, as four float64 arrays."""
+    U = np.ascontiguousarray(U, dtype=np.float64).reshape(-1)
+    if U.size == 0 or U.size % 4:
+        raise ValueError("state must hold 4 values per cell")
+    Path(path).parent.mkdir(parents=True, exist_ok=True)
+    check(lib().o2f_checkpoint_write(str(path).encode(), U.size // 4, _ptr(U), float(time), int(steps)))
+
+
+def load_state_binary(path: str | os.PathLike, n_cells: int) -> tuple[np.ndarray, float, int]:
+    """(state, time, steps) from a binary checkpoint (o2f_checkpoint_read);
+    raises O2FError(O2F_ERR_IO) on a foreign, damaged or mismatched file."""
+    U = np.empty(4 * int(n_cells))
+    t = C.c_double()
+    steps = C.c_int64()
+    check(lib().o2f_checkpoint_read(str(path).encode(), int(n_cells), _ptr(U), C.byref(t), C.byref(steps)))
+    return U, t.value, steps.value
+
+
 def mesh_desc(node_xy, segments, segment_bc, cell_offsets, cell_nodes):
     """Build an o2f_mesh_desc; returns (desc, keepalive)."""
     keep = [np.ascontiguousarray(node_xy, dtype=np.float64).reshape(-1),

@@ -399,6 +399,23 @@ int o2f_set_vertex_coords(o2f_ctx* ctx, const double* node_xy);
  * and outlet vertices fixed; then as o2f_set_vertex_coords. */
 int o2f_deform_shape(o2f_ctx* ctx, const o2f_shape_params* from, const o2f_shape_params* to, int power);
 
+/* Headless counterpart of the reference's live SFML view (Simulator::
+ * output_step, src/simulation.cpp:176-199): the cell scalar of
+ * computeCellScalar (src/compute.cpp:6-60; field "rho", "rho_u", "rho_v",
+ * "E", "u", "v", "p" / "pressure", or from the Green-Gauss gradients of a
+ * residual of the current state "u_x", "u_y", "v_x", "v_y", "div"), drawn
+ * on an nx-by-ny image of the mesh's bounding box, each pixel coloured by
+ * the cell containing its centre (Mesh::computePixelsToCellIDs,
+ * src/mesh.cpp:349-511; black outside the mesh) with colormap_B_W_R, or
+ * colormap_schlieren_bluewhite of sqrt(t) for cmap "schlieren"
+ * (src/renderer_colormap.cpp:10-47).  Colour range: range_in {fmin, fmax},
+ * or with range_in NULL the cells' min and max (for the pressure rounded
+ * outward to multiples of 5000, as output_step does); written to range_out
+ * if not NULL.  rgb_out: nx*ny*3 bytes, top image row first; all black when
+ * fmax <= fmin, as the reference draws nothing then. */
+int o2f_render_field(o2f_ctx* ctx, const char* field, int nx, int ny, const char* cmap, const double* range_in,
+                     uint8_t* rgb_out, double* range_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,8 +7,9 @@ binding.  Importing works without a GPU; creating a ``Solver`` needs one.
 """
 from ._lib import LIB_PATH, O2FError, lib
 from .solver import (Batch, HostMesh, SimulationParams, Solver, load_cell_states, load_config, load_params_generic,
-                     load_state_binary, mesh_desc, save_cell_states, save_state_binary, write_shape_log)
+                     load_state_binary, mesh_desc, save_cell_states, save_state_binary, write_image,
+                     write_shape_log)
 
 __all__ = ["LIB_PATH", "O2FError", "lib", "Batch", "HostMesh", "SimulationParams", "Solver", "load_cell_states",
            "load_config", "load_params_generic", "load_state_binary", "mesh_desc", "save_cell_states",
-           "save_state_binary", "write_shape_log"]
+           "save_state_binary", "write_image", "write_shape_log"]

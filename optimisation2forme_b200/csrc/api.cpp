@@ -502,6 +502,15 @@ int o2f_deform_shape(o2f_ctx* ctx, const o2f_shape_params* from, const o2f_shape
   });
 }
 
+int o2f_render_field(o2f_ctx* ctx, const char* field, int nx, int ny, const char* cmap, const double* range_in,
+                     uint8_t* rgb_out, double* range_out) {
+  return guarded([&] {
+    need(field, "field");
+    need(rgb_out, "rgb_out");
+    S(ctx).render_field(field, nx, ny, cmap ? cmap : "", range_in, rgb_out, range_out);
+  });
+}
+
 int o2f_get_timing(const o2f_ctx* ctx, o2f_timing* t) {
   return guarded([&] {
     need(t, "timing");

@@ -10,6 +10,7 @@
 
 #include "deform.cuh"
 #include "ilu.cuh"
+#include "render.cuh"
 #include "kernels_adjoint.cuh"
 
 namespace o2f {
@@ -414,6 +415,85 @@ void Solver::deform_shape(const o2f_shape_params& from, const o2f_shape_params& 
     xy[2 * vperm_[v] + 1] = moved[v].b;
   }
   set_vertex_coords(xy.data());
+}
+
+void Solver::render_field(const std::string& field, int nx, int ny, const std::string& cmap, const double* range_in,
+                          unsigned char* rgb, double* range_out) {
+  static const char* names[] = {"rho", "rho_u", "rho_v", "E", "u", "v", "u_x", "u_y", "v_x", "v_y", "div", "p"};
+  int f = -1;
+  for (int k = 0; k < 12; ++k)
+    if (field == names[k]) f = k;
+  if (field == "pressure") f = kFieldP;
+  if (f < 0) throw Error(O2F_ERR_ARG, "unknown field '" + field + "' (computeCellScalar)");
+  if (nx <= 0 || ny <= 0 || (int64_t)nx * ny > (int64_t)1 << 28) throw Error(O2F_ERR_ARG, "image size out of range");
+  if (!rgb) throw Error(O2F_ERR_ARG, "null image");
+  const int64_t nc = topo_.nc, npix = (int64_t)nx * ny;
+  cudaStream_t s = stream_;
+  // the gradient fields read the Green-Gauss gradients of a residual of the current state
+  const bool needs_grad = f >= kFieldUx && f <= kFieldDiv;
+  if (needs_grad) {
+    launch_residual(geom_, work_, U_, nullptr, true, nullptr);
+    have_residual_ = true;
+  }
+  if (!render_ref_id_) {
+    std::vector<int32_t> ids(nc);
+    for (int64_t c = 0; c < nc; ++c) ids[c] = (int32_t)cperm_[c];
+    render_ref_id_ = arena_.alloc<int32_t>(nc);
+    render_scalar_ = arena_.alloc<double>(nc);
+    render_part_ = arena_.alloc<double>(2 * 1184);
+    h2d(render_ref_id_, ids, s);
+  }
+  k_cell_scalar<<<grid(nc), kBlock, 0, s>>>(nc, U_, work_.grad, f, params_.gamma, render_scalar_);
+  const int parts = std::min(grid(nc), 1184);
+  k_scalar_minmax<<<parts, kBlock, 0, s>>>(nc, render_scalar_, render_part_);
+  std::vector<double> part(2 * parts);
+  O2F_CUDA(cudaMemcpyAsync(part.data(), render_part_, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  // view: the bounding box of the vertices (Mesh::Mesh, src/mesh.cpp:27-44)
+  double x_min = INFINITY, x_max = -INFINITY, y_min = INFINITY, y_max = -INFINITY;
+  for (int64_t v = 0; v < hm_.nv; ++v) {
+    x_min = std::min(x_min, hm_.vx[v]);
+    x_max = std::max(x_max, hm_.vx[v]);
+    y_min = std::min(y_min, hm_.vy[v]);
+    y_max = std::max(y_max, hm_.vy[v]);
+  }
+  sync();
+  double smin = INFINITY, smax = -INFINITY;
+  for (int k = 0; k < parts; ++k) {
+    if (smin > part[2 * k]) smin = part[2 * k];
+    if (smax < part[2 * k + 1]) smax = part[2 * k + 1];
+  }
+  double fmin_ = smin, fmax_ = smax;
+  if (range_in) {
+    fmin_ = range_in[0];
+    fmax_ = range_in[1];
+  } else if (f == kFieldP) {
+    // Simulator::output_step (src/simulation.cpp:188-193): pressure range in steps of 5000
+    const double step = 5000.0;
+    fmin_ = std::floor(smin / step) * step;
+    fmax_ = std::ceil(smax / step) * step;
+  }
+  if (range_out) {
+    range_out[0] = fmin_;
+    range_out[1] = fmax_;
+  }
+  const double span = fmax_ - fmin_;
+  std::memset(rgb, 0, 3 * (size_t)npix);
+  if (!(span > 0.0)) return;  // render_scalar_field_unstructured draws nothing
+  unsigned long long* pix = nullptr;
+  unsigned char* img = nullptr;
+  O2F_CUDA(cudaMallocAsync(&pix, npix * sizeof(unsigned long long), s));
+  O2F_CUDA(cudaMallocAsync(&img, 3 * npix, s));
+  RenderView w{x_min, y_min, std::abs(x_max - x_min), std::abs(y_max - y_min), nx, ny};
+  O2F_CUDA(cudaMemsetAsync(pix, 0xff, npix * sizeof(unsigned long long), s));
+  k_raster_cells<<<grid(nc), kBlock, 0, s>>>(nc, topo_.cverts, topo_.ctype, geom_.vxy, render_ref_id_, w, pix);
+  k_colour_pixels<<<(int)((npix + kBlock - 1) / kBlock), kBlock, 0, s>>>(nx, ny, pix, render_scalar_, fmin_, span,
+                                                                         cmap == "schlieren" ? 1 : 0, img);
+  O2F_CUDA(cudaGetLastError());
+  O2F_CUDA(cudaMemcpyAsync(rgb, img, 3 * npix, cudaMemcpyDeviceToHost, s));
+  O2F_CUDA(cudaFreeAsync(pix, s));
+  O2F_CUDA(cudaFreeAsync(img, s));
+  sync();
+  launches_ += 4;
 }
 
 // Reverse Cuthill-McKee order of the cell adjacency graph (BFS from a

@@ -80,6 +80,9 @@ class Solver {
   // Wall to the shape `to` by the perturbation formula, interior by inverse
   // distance weighting of the boundary displacements (deform.cuh).
   void deform_shape(const o2f_shape_params& from, const o2f_shape_params& to, int power);
+  // Headless image of a cell field (render.cuh); rgb: nx*ny*3 bytes, top row first.
+  void render_field(const std::string& field, int nx, int ny, const std::string& cmap, const double* range_in,
+                    unsigned char* rgb, double* range_out);
   double last_residual_ms() const { return last_residual_ms_; }
   int64_t launches() const { return launches_; }
 
@@ -164,6 +167,9 @@ class Solver {
   int64_t n_idw_src_ = 0;
   int32_t* idw_src_ = nullptr;
   Vec2<double>*idw_sxy_ = nullptr, *idw_sd_ = nullptr, *dvxy_ = nullptr;
+  // field images
+  int32_t* render_ref_id_ = nullptr;
+  double *render_scalar_ = nullptr, *render_part_ = nullptr;
   double last_residual_ms_ = 0.0;
   int64_t launches_ = 0;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;

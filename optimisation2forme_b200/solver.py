@@ -185,6 +185,27 @@ def _ptr(a: np.ndarray, ct=C.c_double):
     return a.ctypes.data_as(C.POINTER(ct))
 
 
+def write_image(path: str | os.PathLike, img: np.ndarray) -> None:
+    """An RGB uint8 image [h, w, 3] as binary PPM (".ppm") or PNG (other
+    suffixes; zlib, no other dependency)."""
+    import struct
+    import zlib
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape[:2]
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    if path.suffix.lower() == ".ppm":
+        path.write_bytes(f"P6\n{w} {h}\n255\n".encode() + img.tobytes())
+        return
+
+    def chunk(tag: bytes, data: bytes) -> bytes:
+        return struct.pack(">I", len(data)) + tag + data + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+
+    raw = b"".join(b"\x00" + img[r].tobytes() for r in range(h))
+    path.write_bytes(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)) +
+                     chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
+
+
 def save_state_binary(path: str | os.PathLike, U: np.ndarray, time: float = 0.0, steps: int = 0) -> None:
     """Binary checkpoint of a state (o2f_checkpoint_write): the values of the
     reference's text state file, bit for bit, as four float64 arrays."""
@@ -330,6 +351,17 @@ class Solver:
         by the reference's perturbation formula, interior by inverse distance
         weighting with weights |r|^-power."""
         check(lib().o2f_deform_shape(self._h, C.byref(frm), C.byref(to), int(power)))
+
+    def render_field(self, field: str = "p", nx: int = 512, ny: int = 512, cmap: str = "",
+                     vrange: tuple[float, float] | None = None) -> tuple[np.ndarray, tuple[float, float]]:
+        """Headless image of a cell field (o2f_render_field): uint8 [ny, nx, 3],
+        top row first, and the colour range used."""
+        img = np.zeros((int(ny), int(nx), 3), dtype=np.uint8)
+        rng_out = np.zeros(2)
+        rng_in = None if vrange is None else np.asarray(vrange, dtype=np.float64)
+        check(lib().o2f_render_field(self._h, field.encode(), int(nx), int(ny), cmap.encode(),
+                                     None if rng_in is None else _ptr(rng_in), _ptr(img, C.c_uint8), _ptr(rng_out)))
+        return img, (float(rng_out[0]), float(rng_out[1]))
 
     def get_state(self) -> np.ndarray:
         U = np.empty(4 * self.n_cells)

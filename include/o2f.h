@@ -151,6 +151,14 @@ const char* o2f_version(void);
  * recordEdge (:288-297).  Export names: see o2f_mesh_export. */
 int o2f_host_mesh_create(const o2f_mesh_desc* mesh, o2f_host_mesh** out);
 int o2f_host_mesh_from_msh(const char* path, o2f_host_mesh** out);
+
+/* No counterpart in the reference.  As o2f_host_mesh_create, with the
+ * integer topology built on the GPU on `stream` (NULL: the default stream):
+ * the std::map edge order by a stable radix sort of the (vmin, vmax) keys,
+ * the std::unordered_set iteration orders of Vertex::cellIDs, Cell::edgeIDs
+ * and Cell::neighbourIDs by emulation (valence up to 257); geometry and
+ * weights on the host.  Every exported array equals o2f_host_mesh_create's. */
+int o2f_host_mesh_create_gpu(const o2f_mesh_desc* mesh, void* stream, o2f_host_mesh** out);
 int o2f_host_mesh_export(const o2f_host_mesh* mesh, const char* which, void* out, int64_t* count);
 int o2f_host_mesh_destroy(o2f_host_mesh* mesh);
 

@@ -108,6 +108,7 @@ SIGNATURES = {
     "o2f_params_default": ([C.POINTER(Params)], None),
     "o2f_host_mesh_create": ([C.POINTER(MeshDesc), C.POINTER(_vp)], C.c_int),
     "o2f_host_mesh_from_msh": ([C.c_char_p, C.POINTER(_vp)], C.c_int),
+    "o2f_host_mesh_create_gpu": ([C.POINTER(MeshDesc), _vp, C.POINTER(_vp)], C.c_int),
     "o2f_host_mesh_export": ([_vp, C.c_char_p, _vp, _ip], C.c_int),
     "o2f_host_mesh_destroy": ([_vp], C.c_int),
     "o2f_create": ([C.POINTER(MeshDesc), C.POINTER(Params), _vp, C.POINTER(_vp)], C.c_int),

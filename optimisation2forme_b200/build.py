@@ -73,7 +73,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     nvcc = _nvcc()
     BUILD.mkdir(exist_ok=True)
     inc = [f"-I{INCLUDE}", f"-I{CSRC}"]
-    host_flags = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
+    host_flags = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp", "-Wall", "-Wno-unused-function"]
     cuda_inc = ["-I/usr/local/cuda/include"]
     objs = []
     jobs = []
@@ -110,7 +110,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         raise RuntimeError("compilation of libo2f failed")
     if force or jobs or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         _run([nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt", "-ldl",
-              "-lpthread"], verbose)
+              "-lpthread", "-lgomp"], verbose)
     return LIB
 
 

@@ -146,6 +146,25 @@ int o2f_host_mesh_from_msh(const char* path, o2f_host_mesh** out) {
   });
 }
 
+int o2f_host_mesh_create_gpu(const o2f_mesh_desc* mesh, void* stream, o2f_host_mesh** out) {
+  return guarded([&] {
+    need(mesh, "mesh");
+    need(out, "out");
+    *out = nullptr;
+    auto m = std::make_unique<o2f_host_mesh>();
+    try {
+      m->mesh = o2f::build_mesh_gpu(*mesh, stream);
+    } catch (const std::invalid_argument&) {
+      throw;
+    } catch (const o2f::Error&) {
+      throw;
+    } catch (const std::runtime_error& e) {
+      throw o2f::Error(O2F_ERR_MESH, e.what());
+    }
+    *out = m.release();
+  });
+}
+
 int o2f_host_mesh_export(const o2f_host_mesh* mesh, const char* which, void* out, int64_t* count) {
   return guarded([&] {
     need(mesh, "mesh");

@@ -76,22 +76,60 @@ void edge_geometry(HostMesh& m, int64_t e) {
 
 // Vertex::cellIDsOrdered: the cells of every vertex sorted by the angle of
 // their centre about the vertex (src/mesh.cpp:238-247).
+// Vertices are independent: threads split them, with the same result.
 void vertex_cell_order(HostMesh& m) {
-  m.vert_cells_ord.clear();
-  m.vert_cells_ord.reserve(m.vert_cells.size());
-  std::vector<std::pair<double, int64_t>> tmp;
-  for (int64_t v = 0; v < m.nv; ++v) {
-    tmp.clear();
-    for (int64_t k = m.vert_coff[v]; k < m.vert_coff[v + 1]; ++k) {
-      const int64_t c = m.vert_cells[k];
-      tmp.emplace_back(std::atan2(m.ccy[c] - m.vy[v], m.ccx[c] - m.vx[v]), c);
+  m.vert_cells_ord.assign(m.vert_cells.size(), 0);
+#pragma omp parallel
+  {
+    std::vector<std::pair<double, int64_t>> tmp;
+#pragma omp for schedule(static)
+    for (int64_t v = 0; v < m.nv; ++v) {
+      tmp.clear();
+      for (int64_t k = m.vert_coff[v]; k < m.vert_coff[v + 1]; ++k) {
+        const int64_t c = m.vert_cells[k];
+        tmp.emplace_back(std::atan2(m.ccy[c] - m.vy[v], m.ccx[c] - m.vx[v]), c);
+      }
+      std::sort(tmp.begin(), tmp.end(), [](auto& a, auto& b) { return a.first < b.first; });
+      int64_t o = m.vert_coff[v];
+      for (auto& pr : tmp) m.vert_cells_ord[o++] = pr.second;
     }
-    std::sort(tmp.begin(), tmp.end(), [](auto& a, auto& b) { return a.first < b.first; });
-    for (auto& pr : tmp) m.vert_cells_ord.push_back(pr.second);
   }
 }
 
 }  // namespace
+
+std::map<std::pair<int64_t, int64_t>, uint8_t> boundary_segments(const o2f_mesh_desc& d, HostMesh& m) {
+  // Boundary segments (src/mesh.cpp:76-109): the edge code is keyed by
+  // (vmin, vmax); both vertices take the code; later segments win.
+  std::map<std::pair<int64_t, int64_t>, uint8_t> bc;
+  for (int64_t s = 0; s < d.n_segments; ++s) {
+    int64_t a = d.segments[2 * s], b = d.segments[2 * s + 1];
+    if (a < 0 || b < 0 || a >= m.nv || b >= m.nv) throw MeshError("boundary segment vertex out of range");
+    uint8_t code = d.segment_bc[s];
+    if (code != 'i' && code != 'o' && code != 'f' && code != 'w') throw MeshError("unknown boundary code");
+    bc[{std::min(a, b), std::max(a, b)}] = code;
+    m.vbc[a] = code;
+    m.vbc[b] = code;
+  }
+  return bc;
+}
+
+void finish_geometry(HostMesh& m) {
+  m.cvol.resize(m.nc);
+  m.ccx.resize(m.nc);
+  m.ccy.resize(m.nc);
+  m.elen.resize(m.ne);
+  m.enx.resize(m.ne);
+  m.eny.resize(m.ne);
+  m.ecx.resize(m.ne);
+  m.ecy.resize(m.ne);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < m.nc; ++c) cell_geometry(m, c);
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < m.ne; ++e) edge_geometry(m, e);
+  vertex_cell_order(m);
+  compute_vertex_weights(m);
+}
 
 HostMesh build_mesh(const o2f_mesh_desc& d) {
   if (d.n_nodes <= 0 || d.n_cells <= 0 || !d.node_xy || !d.cell_offsets || !d.cell_nodes)
@@ -108,18 +146,7 @@ HostMesh build_mesh(const o2f_mesh_desc& d) {
     m.vx[i] = d.node_xy[2 * i];
     m.vy[i] = d.node_xy[2 * i + 1];
   }
-  // Boundary segments (src/mesh.cpp:76-109): the edge code is keyed by
-  // (vmin, vmax); both vertices take the code; later segments win.
-  std::map<std::pair<int64_t, int64_t>, uint8_t> bc;
-  for (int64_t s = 0; s < d.n_segments; ++s) {
-    int64_t a = d.segments[2 * s], b = d.segments[2 * s + 1];
-    if (a < 0 || b < 0 || a >= m.nv || b >= m.nv) throw MeshError("boundary segment vertex out of range");
-    uint8_t code = d.segment_bc[s];
-    if (code != 'i' && code != 'o' && code != 'f' && code != 'w') throw MeshError("unknown boundary code");
-    bc[{std::min(a, b), std::max(a, b)}] = code;
-    m.vbc[a] = code;
-    m.vbc[b] = code;
-  }
+  const std::map<std::pair<int64_t, int64_t>, uint8_t> bc = boundary_segments(d, m);
   // Cells (src/mesh.cpp:112-177).
   std::map<std::pair<int64_t, int64_t>, std::pair<int64_t, int64_t>> edge_map;
   std::vector<std::unordered_set<std::size_t>> vcells(m.nv);
@@ -248,7 +275,9 @@ void set_coordinates(HostMesh& m, const double* xy) {
       throw MeshError("the new coordinates fold or collapse cell " + std::to_string(c));
     }
   }
+#pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < m.nc; ++c) cell_geometry(m, c);
+#pragma omp parallel for schedule(static)
   for (int64_t e = 0; e < m.ne; ++e) edge_geometry(m, e);
   vertex_cell_order(m);
   compute_vertex_weights(m);
@@ -257,7 +286,11 @@ void set_coordinates(HostMesh& m, const double* xy) {
 void compute_vertex_weights(HostMesh& m) {
   m.vert_wcells.assign(m.vert_cells.size(), 0);
   m.vert_w.assign(m.vert_cells.size(), 0.0);
+  // vertices are independent: threads split them, with the same result
+#pragma omp parallel
+  {
   std::vector<double> w, d, ux, uy;
+#pragma omp for schedule(static)
   for (int64_t v = 0; v < m.nv; ++v) {
     const int64_t o = m.vert_coff[v], n = m.vert_coff[v + 1] - o;
     const double px = m.vx[v], py = m.vy[v];
@@ -325,6 +358,7 @@ void compute_vertex_weights(HostMesh& m) {
       }
     }
   }
+  }  // omp parallel
 }
 
 double min_cell_h(const HostMesh& m) {

@@ -4,7 +4,9 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "o2f.h"
@@ -35,6 +37,20 @@ struct HostMesh {
 };
 
 HostMesh build_mesh(const o2f_mesh_desc& desc);
+
+// The same mesh with the integer topology built on the GPU (topo_gpu.cu):
+// the edge order of the reference's std::map by a stable radix sort of the
+// (vmin, vmax) keys, and the iteration orders of its std::unordered_set
+// members by emulation (uset_order.h); geometry and weights on the host as
+// in build_mesh.  Equal to build_mesh's result array for array.
+HostMesh build_mesh_gpu(const o2f_mesh_desc& desc, void* stream);
+
+// Pieces shared by the two builds.  boundary_segments validates the
+// segments, sets the vertex codes and returns the edge codes by (vmin, vmax)
+// (later segments win); finish_geometry fills every geometric array of a
+// mesh whose topology and coordinates are set.
+std::map<std::pair<int64_t, int64_t>, uint8_t> boundary_segments(const o2f_mesh_desc& d, HostMesh& m);
+void finish_geometry(HostMesh& m);
 
 // New vertex coordinates (xy[2*v], xy[2*v+1] in file order) for a built mesh
 // of the same topology: every geometric quantity (cell volumes and centres,

@@ -56,14 +56,6 @@ void validate_params(const o2f_params& p) {
 
 Solver::Solver(const o2f_mesh_desc& desc, const o2f_params& p, cudaStream_t stream) {
   validate_params(p);
-  try {
-    hm_ = build_mesh(desc);
-  } catch (const std::invalid_argument& e) {
-    throw Error(O2F_ERR_ARG, e.what());
-  } catch (const std::runtime_error& e) {
-    throw Error(O2F_ERR_MESH, e.what());
-  }
-  if (hm_.nc >= (int64_t(1) << 30) || hm_.ne >= (int64_t(1) << 30)) throw Error(O2F_ERR_MESH, "mesh too large");
   int dev_count = 0;
   O2F_CUDA(cudaGetDeviceCount(&dev_count));
   if (stream) {
@@ -72,6 +64,33 @@ Solver::Solver(const o2f_mesh_desc& desc, const o2f_params& p, cudaStream_t stre
     O2F_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     own_stream_ = true;
   }
+  // Large meshes: integer topology on the GPU (the same mesh, array for
+  // array; topo_gpu.cu), unless a vertex has more cells than its set
+  // emulation handles.
+  try {
+    bool built = false;
+    if (desc.n_cells >= kGpuTopologyCells) {
+      try {
+        hm_ = build_mesh_gpu(desc, stream_);
+        built = true;
+      } catch (const TopologyLimit&) {
+      }
+    }
+    if (!built) hm_ = build_mesh(desc);
+  } catch (...) {
+    // the destructor does not run for a failed constructor
+    if (own_stream_) cudaStreamDestroy(stream_);
+    try {
+      throw;
+    } catch (const Error&) {
+      throw;
+    } catch (const std::invalid_argument& e) {
+      throw Error(O2F_ERR_ARG, e.what());
+    } catch (const std::runtime_error& e) {
+      throw Error(O2F_ERR_MESH, e.what());
+    }
+  }
+  if (hm_.nc >= (int64_t(1) << 30) || hm_.ne >= (int64_t(1) << 30)) throw Error(O2F_ERR_MESH, "mesh too large");
   O2F_CUDA(cudaEventCreate(&ev0_));
   O2F_CUDA(cudaEventCreate(&ev1_));
   params_ = p;

@@ -23,6 +23,15 @@ struct Error : std::runtime_error {
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// A mesh beyond what the GPU topology build handles (a vertex with more
+// cells than the set emulation); the host build takes it.
+struct TopologyLimit : Error {
+  using Error::Error;
+};
+
+// Meshes from this many cells up build their topology on the GPU.
+constexpr int64_t kGpuTopologyCells = 100000;
+
 void cuda_check(cudaError_t e, const char* what);
 #define O2F_CUDA(x) ::o2f::cuda_check((x), #x)
 

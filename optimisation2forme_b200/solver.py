@@ -254,10 +254,16 @@ class HostMesh:
     """Host-only mesh build (topology, geometry, interpolation weights) in
     reference order; needs no GPU."""
 
-    def __init__(self, msh: str | os.PathLike | None = None, *, desc=None):
+    def __init__(self, msh: str | os.PathLike | None = None, *, desc=None, gpu: bool = False,
+                 stream: int | None = None):
+        """gpu=True builds the integer topology on the GPU
+        (o2f_host_mesh_create_gpu); the result is the same mesh."""
         h = C.c_void_p()
         if msh is not None:
             check(lib().o2f_host_mesh_from_msh(str(msh).encode(), C.byref(h)))
+        elif gpu:
+            d, self._keep = desc
+            check(lib().o2f_host_mesh_create_gpu(C.byref(d), C.c_void_p(stream) if stream else None, C.byref(h)))
         else:
             d, self._keep = desc
             check(lib().o2f_host_mesh_create(C.byref(d), C.byref(h)))

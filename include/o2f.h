@@ -80,6 +80,17 @@ typedef enum o2f_status {
 #define O2F_DT_REFERENCE 0
 #define O2F_DT_THERMAL 1
 
+/* Operator of the adjoint.  REFERENCE is the reference's: J^T of the
+ * first-order HLLC flux by finite differences and the inviscid wall-pressure
+ * right-hand side (applyJacobianTranspose / assembleAdjointRHS,
+ * src/shape_optimization.cpp:237-554).  FULL is the consistent adjoint: the
+ * Jacobian of the whole residual (reconstruction, limiter, diffusion,
+ * boundary conditions) by coloured central differences about the current
+ * state, stored as 4x4 blocks, and dJ/dU of the whole objective (pressure and
+ * wall stresses) by the same perturbations.  It changes the results. */
+#define O2F_JAC_REFERENCE 0
+#define O2F_JAC_FULL 1
+
 /* Arithmetic of the residual / Jacobian-transpose kernels. */
 #define O2F_PREC_F64 0 /* FP64 throughout (parity mode)                           */
 #define O2F_PREC_F32 1 /* FP32 residual and JT, FP64 reductions, dt and Krylov     */
@@ -110,6 +121,10 @@ typedef struct o2f_params {
   int dt_mode;            /* NEW: O2F_DT_* diffusive time-step bound             */
   int verbosity;        /* >= 1: "[adjoint] iters=.. relres=.." per restart chunk
                              on stderr, as src/shape_optimization.cpp:719 prints */
+  int adjoint_jacobian;   /* NEW: O2F_JAC_* operator and right-hand side of the
+                             adjoint (default REFERENCE)                        */
+  double adjoint_fd_step; /* NEW: relative step of the FULL Jacobian's central
+                             differences (default 1e-9)                         */
 } o2f_params;
 
 void o2f_params_default(o2f_params* p);

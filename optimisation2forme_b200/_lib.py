@@ -58,6 +58,8 @@ class Params(C.Structure):
         ("adjoint_precond", C.c_int),
         ("dt_mode", C.c_int),
         ("verbosity", C.c_int),
+        ("adjoint_jacobian", C.c_int),
+        ("adjoint_fd_step", C.c_double),
     ]
 
 

@@ -106,6 +106,8 @@ void o2f_params_default(o2f_params* p) {
   p->adjoint_precond = O2F_PRECOND_ILU0;
   p->dt_mode = O2F_DT_REFERENCE;
   p->verbosity = 0;
+  p->adjoint_jacobian = O2F_JAC_REFERENCE;
+  p->adjoint_fd_step = 1e-9;
 }
 
 int o2f_host_mesh_create(const o2f_mesh_desc* mesh, o2f_host_mesh** out) {

@@ -198,7 +198,7 @@ void Batch::tune(int reps, int* cfg_out) {
   }
   for (Solver* s : s_) {
     s->have_residual_ = true;
-    s->blk_valid_ = false;
+    s->invalidate_linearisation();
   }
   if (cfg_out)
     for (int p = 0; p < kBatchPhases; ++p) {
@@ -265,7 +265,7 @@ void Batch::rk3_run(int64_t max_steps, double drop_tol, int64_t* steps_done, dou
     if (t_out) t_out[i] = host[i].t;
     if (status) status[i] = host[i].stop == 2 ? O2F_ERR_NONFINITE : O2F_OK;
     s.have_residual_ = host[i].step > 0;
-    s.blk_valid_ = false;
+    s.invalidate_linearisation();
   }
 }
 

@@ -130,7 +130,7 @@ void Solver::residual_norm_noalloc(double* norm_out) {
   const NormScratch sc = norm_scratch();
   launch_residual(geom_, work_, U_, nullptr, true, nullptr);
   have_residual_ = true;
-  blk_valid_ = false;
+  invalidate_linearisation();
   const int blocks = (int)((nc + kNormCellsPerBlock - 1) / kNormCellsPerBlock);
   k_rrho_norm_noalloc<<<blocks, kNormBlock, 0, stream_>>>(work_.R, nc, sc);
   O2F_CUDA(cudaGetLastError());

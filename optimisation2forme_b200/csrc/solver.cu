@@ -10,6 +10,7 @@
 
 #include "deform.cuh"
 #include "ilu.cuh"
+#include "jacobian.cuh"
 #include "render.cuh"
 #include "kernels_adjoint.cuh"
 
@@ -49,6 +50,9 @@ void validate_params(const o2f_params& p) {
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
   if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
+  if (p.adjoint_jacobian != O2F_JAC_REFERENCE && p.adjoint_jacobian != O2F_JAC_FULL)
+    throw Error(O2F_ERR_ARG, "unknown adjoint_jacobian");
+  if (!(p.adjoint_fd_step > 0.0) || !(p.adjoint_fd_step < 1.0)) throw Error(O2F_ERR_ARG, "adjoint_fd_step out of range");
   if (!(p.adjoint_shift >= 0.0) || !(p.adjoint_shift < 1e6)) throw Error(O2F_ERR_ARG, "adjoint_shift out of range");
 }
 
@@ -151,7 +155,7 @@ void Solver::set_params(const o2f_params& p) {
   compute_phys();
   k_venkat_eps<double><<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, p.limiter_k, geom_.cgeom);
   O2F_CUDA(cudaGetLastError());
-  blk_valid_ = false;
+  invalidate_linearisation();
   f32_geom_valid_ = false;  // the FP32 geometry copy holds the old limiter eps
 }
 
@@ -637,8 +641,11 @@ void Solver::ilu_factor() {
     ilu_alloc_ = true;
   }
   O2F_CUDA(cudaMemsetAsync(ilu_status_, 0, sizeof(int), s));
-  k_ilu_assemble<<<grid(nc), kBlock, 0, s>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_,
-                                             params_.adjoint_shift, ilu_);
+  if (full_jac())  // ILU(0) of the full operator on the first-order pattern
+    k_ilu_assemble_full<<<grid(nc), kBlock, 0, s>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, params_.adjoint_shift, ilu_);
+  else
+    k_ilu_assemble<<<grid(nc), kBlock, 0, s>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_,
+                                               params_.adjoint_shift, ilu_);
   for (int l = 0; l < ilu_.n_lo; ++l) {
     const int n = lo_off_h_[l + 1] - lo_off_h_[l];
     k_ilu_factor<<<(n + 127) / 128, 128, 0, s>>>(ilu_.lo_cells + lo_off_h_[l], n, ilu_, ilu_status_);
@@ -741,7 +748,7 @@ void Solver::to_reference(const Vec4<double>* dev, double* ref) {
 void Solver::state_set(const double* U_ref) {
   to_internal(U_ref, U_);
   have_residual_ = false;
-  blk_valid_ = false;
+  invalidate_linearisation();
 }
 
 void Solver::state_get(double* U_ref) { to_reference(U_, U_ref); }
@@ -752,7 +759,7 @@ void Solver::state_freestream() {
       topo_.nc, Vec4<double>{phys_.fs_rho, phys_.fs_rhou, phys_.fs_rhov, phys_.fs_E}, U_);
   O2F_CUDA(cudaGetLastError());
   have_residual_ = false;
-  blk_valid_ = false;
+  invalidate_linearisation();
 }
 
 void Solver::cell_permutation(int64_t* new_of_old) const {
@@ -803,7 +810,7 @@ void Solver::residual(double* R_ref) {
   O2F_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
   last_residual_ms_ = ms;
   have_residual_ = true;
-  blk_valid_ = false;
+  invalidate_linearisation();
   if (R_ref) to_reference(work_.R, R_ref);
 }
 
@@ -815,7 +822,7 @@ void Solver::profile_kernels(int reps, double* ms_out) {
   cudaStream_t s = stream_;
   launch_residual(geom_, work_, U_, nullptr, false, nullptr);  // fresh interface states
   have_residual_ = true;
-  blk_valid_ = false;
+  invalidate_linearisation();
   build_jt_blocks();
   if (!tmp_) tmp_ = arena_.alloc<Vec4<double>>(topo_.nc);
   if (!s_) s_ = arena_.alloc<Vec4<double>>(topo_.nc);
@@ -1009,7 +1016,7 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
     sync();
   }
   have_residual_ = fin.step > 0;
-  blk_valid_ = false;
+  invalidate_linearisation();
   if (fin.stop == 2) throw Error(O2F_ERR_NONFINITE, "non-finite state or residual in the time loop");
 }
 
@@ -1034,16 +1041,189 @@ void Solver::build_jt_blocks() {
 }
 
 void Solver::jt_apply_dev(const Vec4<double>* x, Vec4<double>* y) {
-  k_jt_apply<<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, x, y);
+  if (full_jac())
+    k_fjt_apply<<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, fjac_off_, fjac_idx_, fjac_blk_, x, y);
+  else
+    k_jt_apply<<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, x, y);
   O2F_CUDA(cudaGetLastError());
 }
 
+// Stencils (two vertex rings), their colouring, and the wall edges each cell
+// reaches; host work, once per mesh topology.
+void Solver::setup_full_jacobian() {
+  if (fjac_setup_) return;
+  const HostMesh& m = hm_;
+  const int64_t nc = m.nc;
+  // cells sharing a vertex with cell c (device numbering, ascending)
+  std::vector<int64_t> voff(nc + 1, 0);
+  std::vector<int32_t> vcl;
+  std::vector<int64_t> stamp(nc, -1);
+  std::vector<int32_t> tmp;
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t co = cperm_[c];
+    tmp.clear();
+    for (int64_t k = m.cell_voff[co]; k < m.cell_voff[co + 1]; ++k) {
+      const int64_t v = m.cell_verts[k];
+      for (int64_t q = m.vert_coff[v]; q < m.vert_coff[v + 1]; ++q) {
+        const int64_t c2 = cinv_[m.vert_cells[q]];
+        if (stamp[c2] != c) {
+          stamp[c2] = c;
+          tmp.push_back((int32_t)c2);
+        }
+      }
+    }
+    std::sort(tmp.begin(), tmp.end());
+    vcl.insert(vcl.end(), tmp.begin(), tmp.end());
+    voff[c + 1] = (int64_t)vcl.size();
+  }
+  // S(c): two rings
+  std::fill(stamp.begin(), stamp.end(), -1);
+  std::vector<int64_t> soff(nc + 1, 0);
+  std::vector<int32_t> sidx;
+  for (int64_t c = 0; c < nc; ++c) {
+    tmp.clear();
+    for (int64_t a = voff[c]; a < voff[c + 1]; ++a)
+      for (int64_t b = voff[vcl[a]]; b < voff[vcl[a] + 1]; ++b) {
+        const int32_t c2 = vcl[b];
+        if (stamp[c2] != c) {
+          stamp[c2] = c;
+          tmp.push_back(c2);
+        }
+      }
+    std::sort(tmp.begin(), tmp.end());
+    sidx.insert(sidx.end(), tmp.begin(), tmp.end());
+    soff[c + 1] = (int64_t)sidx.size();
+  }
+  // greedy colouring: no two cells of one colour in any S(i)
+  std::vector<int32_t> color(nc, -1);
+  std::vector<int64_t> mark;
+  int32_t ncol = 0;
+  for (int64_t j = 0; j < nc; ++j) {
+    for (int64_t a = soff[j]; a < soff[j + 1]; ++a) {
+      const int32_t i = sidx[a];
+      for (int64_t b = soff[i]; b < soff[i + 1]; ++b) {
+        const int32_t col = color[sidx[b]];
+        if (col >= 0) mark[col] = j;
+      }
+    }
+    int32_t col = 0;
+    while (col < ncol && mark[col] == j) ++col;
+    if (col == ncol) {
+      ++ncol;
+      mark.push_back(-1);
+    }
+    color[j] = col;
+  }
+  fjac_coff_h_.assign(ncol + 1, 0);
+  for (int64_t j = 0; j < nc; ++j) ++fjac_coff_h_[color[j] + 1];
+  for (int32_t c = 0; c < ncol; ++c) fjac_coff_h_[c + 1] += fjac_coff_h_[c];
+  std::vector<int32_t> ccells(nc);
+  std::vector<int64_t> fill(fjac_coff_h_.begin(), fjac_coff_h_.end() - 1);
+  for (int64_t j = 0; j < nc; ++j) ccells[fill[color[j]]++] = (int32_t)j;
+  // wall edges (objective terms) reaching each cell: those of its stencil's owners
+  std::vector<int64_t> wcount(nc + 1, 0);
+  const int64_t nw = (int64_t)wall_edges_host_.size();
+  std::vector<int32_t> wcell(nw);
+  for (int64_t w = 0; w < nw; ++w) {
+    const int64_t eo = eperm_[wall_edges_host_[w]];
+    wcell[w] = (int32_t)cinv_[m.e_cl[eo]];
+    for (int64_t a = soff[wcell[w]]; a < soff[wcell[w] + 1]; ++a) ++wcount[sidx[a] + 1];
+  }
+  for (int64_t j = 0; j < nc; ++j) wcount[j + 1] += wcount[j];
+  std::vector<int32_t> widx(wcount[nc]);
+  std::vector<int64_t> wfill(wcount.begin(), wcount.end() - 1);
+  for (int64_t w = 0; w < nw; ++w)
+    for (int64_t a = soff[wcell[w]]; a < soff[wcell[w] + 1]; ++a) widx[wfill[sidx[a]]++] = (int32_t)w;
+  fjac_nnzb_ = soff[nc];
+  cudaStream_t st = stream_;
+  fjac_off_ = arena_.alloc<int64_t>(nc + 1);
+  fjac_idx_ = arena_.alloc<int32_t>(sidx.size());
+  fjac_ccells_ = arena_.alloc<int32_t>(nc);
+  fjac_woff_ = arena_.alloc<int64_t>(nc + 1);
+  fjac_widx_ = arena_.alloc<int32_t>(std::max<size_t>(widx.size(), 1));
+  h2d(fjac_off_, soff, st);
+  h2d(fjac_idx_, sidx, st);
+  h2d(fjac_ccells_, ccells, st);
+  h2d(fjac_woff_, wcount, st);
+  if (!widx.empty()) h2d(fjac_widx_, widx, st);
+  fjac_blk_ = arena_.alloc<double>(16 * fjac_nnzb_);
+  fjac_gL_ = arena_.alloc<double>(4 * nc);
+  fjac_gD_ = arena_.alloc<double>(4 * nc);
+  fjac_tlp_ = arena_.alloc<double>(std::max<int64_t>(nw, 1));
+  fjac_tdp_ = arena_.alloc<double>(std::max<int64_t>(nw, 1));
+  fjac_tlm_ = arena_.alloc<double>(std::max<int64_t>(nw, 1));
+  fjac_tdm_ = arena_.alloc<double>(std::max<int64_t>(nw, 1));
+  fjac_Up_ = arena_.alloc<Vec4<double>>(nc);
+  fjac_Rp_ = arena_.alloc<Vec4<double>>(nc);
+  sync();
+  fjac_setup_ = true;
+}
+
+// The full Jacobian and dC_L/dU, dC_D/dU about the current state: for every
+// colour and component, two residuals (state +- eps on the colour's cells),
+// then the columns of the blocks and the objective gradient.  Leaves the
+// residual and interface states of the current state in the context.
+void Solver::build_full_jacobian() {
+  if (fjac_valid_) return;
+  setup_full_jacobian();
+  const int64_t nc = topo_.nc, nw = topo_.n_wall;
+  cudaStream_t st = stream_;
+  const Phys& ph = phys_;
+  const double a_inf = std::sqrt(ph.gamma * params_.p_ref / params_.rho_ref);
+  // Steps of 1e-9 relative: the reference's Venkatakrishnan eps = (K h)^3 is
+  // absolute, so for E and rho*u (1e5 and 1e2 in SI units) the limiter turns
+  // over within ~1e-4 absolute on fine cells; larger steps difference across
+  // that turn (1e-6: 2e-2 off the directional derivative, 1e-8: 7e-4,
+  // 1e-10: 2e-5 with roundoff reaching 1e-5 in dJ/dU).
+  FjacEps e{};
+  e.h = params_.adjoint_fd_step;
+  e.floor[0] = 1e-2 * ph.fs_rho;
+  e.floor[1] = 1e-2 * ph.fs_rho * a_inf;
+  e.floor[2] = 1e-2 * ph.fs_rho * a_inf;
+  e.floor[3] = 1e-2 * ph.fs_E;
+  O2F_CUDA(cudaMemsetAsync(fjac_gL_, 0, 4 * nc * sizeof(double), st));
+  O2F_CUDA(cudaMemsetAsync(fjac_gD_, 0, 4 * nc * sizeof(double), st));
+  O2F_CUDA(cudaMemcpyAsync(fjac_Up_, U_, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, st));
+  const int64_t ncol = (int64_t)fjac_coff_h_.size() - 1;
+  for (int64_t col = 0; col < ncol; ++col) {
+    const int32_t* cells = fjac_ccells_ + fjac_coff_h_[col];
+    const int64_t n = fjac_coff_h_[col + 1] - fjac_coff_h_[col];
+    for (int k = 0; k < 4; ++k) {
+      k_fjac_perturb<<<grid(n), kBlock, 0, st>>>(n, cells, U_, fjac_Up_, k, 1.0, e);
+      launch_residual(geom_, work_, fjac_Up_, nullptr, false, nullptr);
+      O2F_CUDA(cudaMemcpyAsync(fjac_Rp_, work_.R, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, st));
+      if (nw) k_fjac_wall_terms<<<grid(nw), kBlock, 0, st>>>(nw, topo_.wall_edges, geom_, work_.eL, work_.etq, ph,
+                                                              fjac_tlp_, fjac_tdp_);
+      k_fjac_perturb<<<grid(n), kBlock, 0, st>>>(n, cells, U_, fjac_Up_, k, -1.0, e);
+      launch_residual(geom_, work_, fjac_Up_, nullptr, false, nullptr);
+      if (nw) k_fjac_wall_terms<<<grid(nw), kBlock, 0, st>>>(nw, topo_.wall_edges, geom_, work_.eL, work_.etq, ph,
+                                                              fjac_tlm_, fjac_tdm_);
+      k_fjac_extract<<<grid(n), kBlock, 0, st>>>(n, cells, fjac_off_, fjac_idx_, U_, fjac_Rp_, work_.R, k, e,
+                                                  fjac_blk_);
+      if (nw)
+        k_fjac_grad_extract<<<grid(n), kBlock, 0, st>>>(n, cells, fjac_woff_, fjac_widx_, U_, fjac_tlp_, fjac_tdp_,
+                                                         fjac_tlm_, fjac_tdm_, k, e, fjac_gL_, fjac_gD_);
+      k_fjac_restore<<<grid(n), kBlock, 0, st>>>(n, cells, U_, fjac_Up_);
+      O2F_CUDA(cudaGetLastError());
+      launches_ += 7;
+    }
+  }
+  // the residual and interface states of the state itself
+  launch_residual(geom_, work_, U_, nullptr, false, nullptr);
+  O2F_CUDA(cudaGetLastError());
+  sync();
+  have_residual_ = true;
+  blk_valid_ = false;  // the first-order blocks follow the interface states just computed
+  fjac_valid_ = true;
+}
+
 void Solver::jt_apply(const double* x_ref, double* y_ref) {
+  if (full_jac()) build_full_jacobian();
   build_jt_blocks();
   if (!tmp_) tmp_ = arena_.alloc<Vec4<double>>(topo_.nc);
   if (!s_) s_ = arena_.alloc<Vec4<double>>(topo_.nc);
   to_internal(x_ref, s_);
-  if (f32()) {
+  if (f32() && !full_jac()) {
     k_jt_apply<<<grid(topo_.nc), kBlock, 0, stream_>>>(topo_.nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, s_,
                                                        tmp_);
     O2F_CUDA(cudaGetLastError());
@@ -1056,6 +1236,14 @@ void Solver::jt_apply(const double* x_ref, double* y_ref) {
 void Solver::adjoint_rhs(double beta, double* b_ref) {
   if (!have_residual_) throw Error(O2F_ERR_STATE, "no residual has been evaluated");
   if (!b_) b_ = arena_.alloc<Vec4<double>>(topo_.nc);
+  if (full_jac()) {  // dJ/dU of the whole objective
+    build_full_jacobian();
+    k_fjac_rhs<<<grid(4 * topo_.nc), kBlock, 0, stream_>>>(4 * topo_.nc, fjac_gL_, fjac_gD_, beta,
+                                                           reinterpret_cast<double*>(b_));
+    O2F_CUDA(cudaGetLastError());
+    if (b_ref) to_reference(b_, b_ref);
+    return;
+  }
   O2F_CUDA(cudaMemsetAsync(b_, 0, topo_.nc * sizeof(Vec4<double>), stream_));
   if (topo_.n_wall_cells > 0)
     k_adjoint_rhs<<<grid(topo_.n_wall_cells), kBlock, 0, stream_>>>(topo_.n_wall_cells, topo_.wall_cells,
@@ -1068,7 +1256,9 @@ void Solver::adjoint_rhs(double beta, double* b_ref) {
 void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
                            int64_t* iters, double* relres_out, const double* guess_ref) {
   if (!(tol > 0.0) || max_iter <= 0 || restart <= 0) throw Error(O2F_ERR_ARG, "invalid solver settings");
-  build_jt_blocks();
+  const bool full = full_jac();
+  if (full) build_full_jacobian();  // first: it recomputes the interface states
+  build_jt_blocks();                // (the preconditioner's blocks in the full mode)
   adjoint_rhs(beta, nullptr);
   const int64_t nc = topo_.nc, n4 = 4 * nc;
   auto need = [&](Vec4<double>*& p) {
@@ -1126,7 +1316,9 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     k_bicg_p<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_),
                                                reinterpret_cast<double*>(p_), reinterpret_cast<double*>(v_), ks_);
     if (precond) ilu_apply(p_, ph, kgate);
-    if (f32())  // FP32 blocks; restarts take the true residual with the FP64 operator
+    if (full)
+      k_bicg_fjt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, ph, v_, r0_, part_, ks_);
+    else if (f32())  // FP32 blocks; restarts take the true residual with the FP64 operator
       k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, ph, v_, r0_,
                                                     part_, ks_);
     else
@@ -1135,7 +1327,9 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     k_bicg_s<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(v_),
                                                reinterpret_cast<double*>(s_), ks_);
     if (precond) ilu_apply(s_, sh, kgate);
-    if (f32())
+    if (full)
+      k_bicg_fjt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, sh, s_, t_, part_, ks_);
+    else if (f32())
       k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, sh, s_, t_,
                                                     part_, ks_);
     else
@@ -1290,7 +1484,7 @@ void Solver::shape_gradient(const o2f_shape_params& sp, const int* ids, int n, d
   // computeShapeGradient starts with a residual of the unperturbed mesh (:955-956).
   launch_residual(geom_, work_, U_, nullptr, false, nullptr);
   have_residual_ = true;
-  blk_valid_ = false;
+  invalidate_linearisation();
   for (int k = 0; k < n; ++k) {
     double J[2];
     for (int sgn = 0; sgn < 2; ++sgn) {

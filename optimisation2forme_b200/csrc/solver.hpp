@@ -102,6 +102,16 @@ class Solver {
   void launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<double>* U, const int* gate,
                        bool write_grad, const void* rk);
   void build_jt_blocks();
+  // Both linearisations (first-order blocks, full Jacobian) belong to the
+  // state, geometry and parameters they were built for.
+  void invalidate_linearisation() {
+    blk_valid_ = false;
+    fjac_valid_ = false;
+  }
+  // consistent adjoint (jacobian.cuh)
+  bool full_jac() const { return params_.adjoint_jacobian == O2F_JAC_FULL; }
+  void setup_full_jacobian();
+  void build_full_jacobian();
   void jt_apply_dev(const Vec4<double>* x, Vec4<double>* y);
   void perturbed_geometry(const o2f_shape_params& sp, int id, double eps);
   void ensure_pert_buffers();
@@ -171,6 +181,15 @@ class Solver {
   Work<double> pwork_{};
   Vec4<double>* Rp_ = nullptr;
   bool pert_alloc_ = false;
+  // consistent adjoint: stencil S(j) (device order), colours, blocks, dC/dU
+  bool fjac_setup_ = false, fjac_valid_ = false;
+  int64_t fjac_nnzb_ = 0;
+  int64_t *fjac_off_ = nullptr, *fjac_woff_ = nullptr;
+  int32_t *fjac_idx_ = nullptr, *fjac_ccells_ = nullptr, *fjac_widx_ = nullptr;
+  std::vector<int64_t> fjac_coff_h_;
+  double *fjac_blk_ = nullptr, *fjac_gL_ = nullptr, *fjac_gD_ = nullptr;
+  double *fjac_tlp_ = nullptr, *fjac_tdp_ = nullptr, *fjac_tlm_ = nullptr, *fjac_tdm_ = nullptr;
+  Vec4<double>*fjac_Up_ = nullptr, *fjac_Rp_ = nullptr;
   // mesh deformation
   bool deform_alloc_ = false;
   int64_t n_idw_src_ = 0;

@@ -58,6 +58,8 @@ class SimulationParams:
     adjoint_precond: str = "ilu0"
     dt_mode: str = "reference"
     adjoint_shift: float = 0.0
+    adjoint_jacobian: str = "reference"
+    adjoint_fd_step: float = 1e-9
     max_steps: int = 2**62
     residual_drop: float = 0.0
     adjoint_tol: float = 1e-6
@@ -68,7 +70,7 @@ class SimulationParams:
         p = _lib.Params()
         lib().o2f_params_default(C.byref(p))
         for f in ("gamma", "viscosity", "Pr", "cp", "cfl_number", "final_time", "inflow_velocity", "rho_ref",
-                  "p_ref", "aoa_deg", "limiter_k", "adjoint_shift"):
+                  "p_ref", "aoa_deg", "limiter_k", "adjoint_shift", "adjoint_fd_step"):
             setattr(p, f, float(getattr(self, f)))
         lim = self.limiter.lower()
         if lim in ("venkatakrishnan", "venkat"):
@@ -80,15 +82,17 @@ class SimulationParams:
         p.precision = {"fp64": _lib.PREC_F64, "fp32": _lib.PREC_F32}[self.precision.lower()]
         p.adjoint_precond = {"none": 0, "identity": 0, "ilu0": 1}[self.adjoint_precond.lower()]
         p.dt_mode = {"reference": 0, "thermal": 1}[self.dt_mode.lower()]
+        p.adjoint_jacobian = {"reference": 0, "first_order": 0, "full": 1}[self.adjoint_jacobian.lower()]
         p.verbosity = int(self.verbosity)
         return p
 
 
 _FLOAT_KEYS = {"cfl_number", "final_time", "gamma", "viscosity", "Pr", "cp", "inflow_velocity", "rho_ref", "p_ref",
-               "aoa_deg", "limiter_k", "residual_drop", "adjoint_tol", "adjoint_shift"}
+               "aoa_deg", "limiter_k", "residual_drop", "adjoint_tol", "adjoint_shift", "adjoint_fd_step"}
 _INT_KEYS = {"verbosity", "max_steps", "adjoint_restart", "adjoint_max_iter"}
 _STR_KEYS = {"mesh_name", "boundary_conditions", "initial_condition", "state_load_path", "state_save_path",
-             "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond", "dt_mode"}
+             "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond", "dt_mode",
+             "adjoint_jacobian"}
 
 
 def load_config(path: str | os.PathLike, params: SimulationParams | None = None) -> SimulationParams:

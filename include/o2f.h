@@ -90,6 +90,10 @@ typedef enum o2f_status {
  * wall stresses) by the same perturbations.  It changes the results. */
 #define O2F_JAC_REFERENCE 0
 #define O2F_JAC_FULL 1
+/* FROZEN: as FULL with the limiter values held at the current state (the
+ * usual linearisation of limited schemes: reconstruction, fluxes, diffusion
+ * and objective differentiated, the limiter's own derivative left out). */
+#define O2F_JAC_FROZEN 2
 
 /* Arithmetic of the residual / Jacobian-transpose kernels. */
 #define O2F_PREC_F64 0 /* FP64 throughout (parity mode)                           */
@@ -272,6 +276,14 @@ int o2f_adjoint_solve(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, i
 /* NEW: o2f_adjoint_solve started from lambda0_host (reference order)
  * instead of zero -- the warm start of the learned predictor.  The solution
  * criterion is unchanged: true relres <= tol. */
+/* No counterpart in the reference.  J^T lambda = rhs (rhs: 4 values per
+ * cell, interleaved, mesh-file cell order) with the context's operator,
+ * preconditioner and stopping rule of o2f_adjoint_solve; lambda0_host may be
+ * NULL (start from zero).  For outer iterations built on the adjoint
+ * operator, e.g. defect correction. */
+int o2f_adjoint_solve_rhs(o2f_ctx* ctx, const double* rhs_host, double tol, int64_t max_iter, int64_t restart,
+                          const double* lambda0_host, double* lambda_host, int64_t* iters, double* relres);
+
 int o2f_adjoint_solve_guess(o2f_ctx* ctx, double beta, double tol, int64_t max_iter, int64_t restart,
                             const double* lambda0_host, double* lambda_host, int64_t* iters, double* relres);
 

@@ -146,6 +146,8 @@ SIGNATURES = {
     "o2f_deform_shape": ([_vp, C.POINTER(ShapeParams), C.POINTER(ShapeParams), C.c_int], C.c_int),
     "o2f_render_field": ([_vp, C.c_char_p, C.c_int, C.c_int, C.c_char_p, _dp, C.POINTER(C.c_uint8), _dp], C.c_int),
     "o2f_batch_create": ([C.POINTER(_vp), C.c_int, C.POINTER(_vp)], C.c_int),
+    "o2f_adjoint_solve_rhs": ([_vp, _dp, C.c_double, C.c_int64, C.c_int64, _dp, _dp, C.POINTER(C.c_int64), _dp],
+                              C.c_int),
     "o2f_adjoint_solve_guess": ([_vp, C.c_double, C.c_double, C.c_int64, C.c_int64, _dp, _dp, C.POINTER(C.c_int64),
                                  _dp], C.c_int),
     "o2f_mlp_create": ([C.c_int, C.c_float, C.c_uint64, _vp, C.POINTER(_vp)], C.c_int),

@@ -332,6 +332,14 @@ int o2f_adjoint_solve_guess(o2f_ctx* ctx, double beta, double tol, int64_t max_i
   });
 }
 
+int o2f_adjoint_solve_rhs(o2f_ctx* ctx, const double* rhs_host, double tol, int64_t max_iter, int64_t restart,
+                          const double* lambda0_host, double* lambda_host, int64_t* iters, double* relres) {
+  return guarded([&] {
+    need(rhs_host, "rhs");
+    S(ctx).adjoint_solve(0.0, tol, max_iter, restart, lambda_host, iters, relres, lambda0_host, rhs_host);
+  });
+}
+
 int o2f_shape_gradient(o2f_ctx* ctx, const o2f_shape_params* shape, const int* param_ids, int n_params, double beta,
                        double eps, const double* lambda_host, double* grad_out) {
   return guarded([&] {

@@ -24,6 +24,19 @@
 
 namespace o2f {
 
+// The gradient phase of the residual with the limiter recorded (kAlpha 1)
+// or held (kAlpha 2); the rest of the residual is launched as usual.
+template <int kAlpha>
+__global__ void __launch_bounds__(kBlock, 3) k_cell_gradient_alpha(
+    int64_t nc, const int32_t* __restrict__ slot, Geom<double> g, const int2* __restrict__ ev,
+    const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<double>* __restrict__ U,
+    const Vec4<double>* __restrict__ vq, Phys ph, Vec4<double>* __restrict__ eL, Vec4<double>* __restrict__ eR,
+    Vec4<double>* __restrict__ ctq, double* __restrict__ ctqy, Vec4<double>* __restrict__ alpha) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  cell_gradient_at<double, false, kAlpha>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, nullptr, alpha);
+}
+
 struct FjacEps {
   double h;         // relative step
   double floor[4];  // absolute floor per component

@@ -281,12 +281,16 @@ __global__ void __launch_bounds__(kBlock) k_vertex_visc(int64_t nv, const int32_
 // reciprocal (qdiv_flag) and returns false, having written nothing, if any
 // quotient left qdiv's range; cell_gradient_at then redoes the cell with
 // kPlain = true (IEEE divisions), out of line.
-template <typename T, bool kWriteGrad, bool kPlain>
+//
+// kAlpha (linearisations only; 0 everywhere else): 1 stores the limiter
+// values of the cell in alpha[c], 2 uses alpha[c] instead of computing them
+// (the limiter held at a base state).
+template <typename T, bool kWriteGrad, bool kPlain, int kAlpha = 0>
 __device__ __forceinline__ bool cell_gradient_body(int64_t c,
     int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
     const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
     const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
-    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad) {
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad, Vec4<T>* __restrict__ alpha = nullptr) {
   const Vec4<T> cg = g.cgeom[c];
   const T cx = cg.a, cy = cg.b, cv = cg.c, veps = cg.d;
   const Vec4<T> u = U[c];
@@ -369,17 +373,34 @@ __device__ __forceinline__ bool cell_gradient_body(int64_t c,
   const int kind = ph.limiter;
   T al0 = (T)1.0, al1 = (T)1.0, al2 = (T)1.0, al3 = (T)1.0;
   T dxk[4], dyk[4];
+  if constexpr (kAlpha == 2) {
+    const Vec4<T> a = alpha[c];
+    al0 = a.a;
+    al1 = a.b;
+    al2 = a.c;
+    al3 = a.d;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k >= nk) continue;
-    const Vec2<T> ce = g.ectr[sl[k] >> 1];
-    const T dx = ce.a - cx, dy = ce.b - cy;
-    dxk[k] = dx;
-    dyk[k] = dy;
-    al0 = smin(al0, limiter_alpha(kind, u.a, u.a + gx0 * dx + gy0 * dy, mn0, mx0, veps));
-    al1 = smin(al1, limiter_alpha(kind, u.b, u.b + gx1 * dx + gy1 * dy, mn1, mx1, veps));
-    al2 = smin(al2, limiter_alpha(kind, u.c, u.c + gx2 * dx + gy2 * dy, mn2, mx2, veps));
-    al3 = smin(al3, limiter_alpha(kind, u.d, u.d + gx3 * dx + gy3 * dy, mn3, mx3, veps));
+    for (int k = 0; k < 4; ++k) {
+      if (k >= nk) continue;
+      const Vec2<T> ce = g.ectr[sl[k] >> 1];
+      dxk[k] = ce.a - cx;
+      dyk[k] = ce.b - cy;
+    }
+    (void)kind;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k >= nk) continue;
+      const Vec2<T> ce = g.ectr[sl[k] >> 1];
+      const T dx = ce.a - cx, dy = ce.b - cy;
+      dxk[k] = dx;
+      dyk[k] = dy;
+      al0 = smin(al0, limiter_alpha(kind, u.a, u.a + gx0 * dx + gy0 * dy, mn0, mx0, veps));
+      al1 = smin(al1, limiter_alpha(kind, u.b, u.b + gx1 * dx + gy1 * dy, mn1, mx1, veps));
+      al2 = smin(al2, limiter_alpha(kind, u.c, u.c + gx2 * dx + gy2 * dy, mn2, mx2, veps));
+      al3 = smin(al3, limiter_alpha(kind, u.d, u.d + gx3 * dx + gy3 * dy, mn3, mx3, veps));
+    }
+    if constexpr (kAlpha == 1) alpha[c] = v4<T>(al0, al1, al2, al3);
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -421,23 +442,26 @@ __device__ __forceinline__ bool cell_gradient_body(int64_t c,
   return true;
 }
 
-template <typename T, bool kWriteGrad>
+template <typename T, bool kWriteGrad, int kAlpha = 0>
 __device__ __noinline__ void cell_gradient_plain(int64_t c,
     int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
     const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
     const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
-    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad) {
-  cell_gradient_body<T, kWriteGrad, true>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad);
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad, Vec4<T>* __restrict__ alpha) {
+  cell_gradient_body<T, kWriteGrad, true, kAlpha>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad,
+                                                  alpha);
 }
 
-template <typename T, bool kWriteGrad>
+template <typename T, bool kWriteGrad, int kAlpha = 0>
 __device__ __forceinline__ void cell_gradient_at(int64_t c,
     int64_t nc, const int32_t* __restrict__ slot, Geom<T> g, const int2* __restrict__ ev,
     const int2* __restrict__ ec, const uint8_t* __restrict__ ebc, const Vec4<T>* __restrict__ U,
     const Vec4<T>* __restrict__ vq, Phys ph, Vec4<T>* __restrict__ eL, Vec4<T>* __restrict__ eR,
-    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad) {
-  if (!cell_gradient_body<T, kWriteGrad, false>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad))
-    cell_gradient_plain<T, kWriteGrad>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad);
+    Vec4<T>* __restrict__ ctq, T* __restrict__ ctqy, Vec4<T>* __restrict__ grad,
+    Vec4<T>* __restrict__ alpha = nullptr) {
+  if (!cell_gradient_body<T, kWriteGrad, false, kAlpha>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad,
+                                                        alpha))
+    cell_gradient_plain<T, kWriteGrad, kAlpha>(c, nc, slot, g, ev, ec, ebc, U, vq, ph, eL, eR, ctq, ctqy, grad, alpha);
 }
 
 template <typename T, bool kWriteGrad>

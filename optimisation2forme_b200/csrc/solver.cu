@@ -50,7 +50,8 @@ void validate_params(const o2f_params& p) {
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
   if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
-  if (p.adjoint_jacobian != O2F_JAC_REFERENCE && p.adjoint_jacobian != O2F_JAC_FULL)
+  if (p.adjoint_jacobian != O2F_JAC_REFERENCE && p.adjoint_jacobian != O2F_JAC_FULL &&
+      p.adjoint_jacobian != O2F_JAC_FROZEN)
     throw Error(O2F_ERR_ARG, "unknown adjoint_jacobian");
   if (!(p.adjoint_fd_step > 0.0) || !(p.adjoint_fd_step < 1.0)) throw Error(O2F_ERR_ARG, "adjoint_fd_step out of range");
   if (!(p.adjoint_shift >= 0.0) || !(p.adjoint_shift < 1e6)) throw Error(O2F_ERR_ARG, "adjoint_shift out of range");
@@ -767,11 +768,17 @@ void Solver::cell_permutation(int64_t* new_of_old) const {
 }
 
 void Solver::launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<double>* U, const int* gate,
-                             bool write_grad, const void* rkp) {
+                             bool write_grad, const void* rkp, int alpha_mode) {
   const Topo& t = topo_;
   cudaStream_t s = stream_;
   k_vertex_state<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, U, phys_, w.vq, gate);
-  if (write_grad)
+  if (alpha_mode == 1)
+    k_cell_gradient_alpha<1><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_, w.eL,
+                                                            w.eR, w.ctq, w.ctqy, fjac_alpha_);
+  else if (alpha_mode == 2)
+    k_cell_gradient_alpha<2><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_, w.eL,
+                                                            w.eR, w.ctq, w.ctqy, fjac_alpha_);
+  else if (write_grad)
     k_cell_gradient<double, true><<<grid(t.nc), kBlock, 0, s>>>(t.nc, t.slot, g, t.ev, t.ec, t.ebc, U, w.vq, phys_,
                                                                 w.eL, w.eR, w.ctq, w.ctqy, w.grad, gate);
   else
@@ -1155,6 +1162,7 @@ void Solver::setup_full_jacobian() {
   fjac_tdm_ = arena_.alloc<double>(std::max<int64_t>(nw, 1));
   fjac_Up_ = arena_.alloc<Vec4<double>>(nc);
   fjac_Rp_ = arena_.alloc<Vec4<double>>(nc);
+  fjac_alpha_ = arena_.alloc<Vec4<double>>(nc);
   sync();
   fjac_setup_ = true;
 }
@@ -1184,18 +1192,22 @@ void Solver::build_full_jacobian() {
   O2F_CUDA(cudaMemsetAsync(fjac_gL_, 0, 4 * nc * sizeof(double), st));
   O2F_CUDA(cudaMemsetAsync(fjac_gD_, 0, 4 * nc * sizeof(double), st));
   O2F_CUDA(cudaMemcpyAsync(fjac_Up_, U_, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, st));
+  // frozen limiter: the limiter values of the current state, held in every
+  // perturbed residual
+  const int amode = params_.adjoint_jacobian == O2F_JAC_FROZEN ? 2 : 0;
+  if (amode) launch_residual(geom_, work_, U_, nullptr, false, nullptr, 1);
   const int64_t ncol = (int64_t)fjac_coff_h_.size() - 1;
   for (int64_t col = 0; col < ncol; ++col) {
     const int32_t* cells = fjac_ccells_ + fjac_coff_h_[col];
     const int64_t n = fjac_coff_h_[col + 1] - fjac_coff_h_[col];
     for (int k = 0; k < 4; ++k) {
       k_fjac_perturb<<<grid(n), kBlock, 0, st>>>(n, cells, U_, fjac_Up_, k, 1.0, e);
-      launch_residual(geom_, work_, fjac_Up_, nullptr, false, nullptr);
+      launch_residual(geom_, work_, fjac_Up_, nullptr, false, nullptr, amode);
       O2F_CUDA(cudaMemcpyAsync(fjac_Rp_, work_.R, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToDevice, st));
       if (nw) k_fjac_wall_terms<<<grid(nw), kBlock, 0, st>>>(nw, topo_.wall_edges, geom_, work_.eL, work_.etq, ph,
                                                               fjac_tlp_, fjac_tdp_);
       k_fjac_perturb<<<grid(n), kBlock, 0, st>>>(n, cells, U_, fjac_Up_, k, -1.0, e);
-      launch_residual(geom_, work_, fjac_Up_, nullptr, false, nullptr);
+      launch_residual(geom_, work_, fjac_Up_, nullptr, false, nullptr, amode);
       if (nw) k_fjac_wall_terms<<<grid(nw), kBlock, 0, st>>>(nw, topo_.wall_edges, geom_, work_.eL, work_.etq, ph,
                                                               fjac_tlm_, fjac_tdm_);
       k_fjac_extract<<<grid(n), kBlock, 0, st>>>(n, cells, fjac_off_, fjac_idx_, U_, fjac_Rp_, work_.R, k, e,
@@ -1254,12 +1266,17 @@ void Solver::adjoint_rhs(double beta, double* b_ref) {
 }
 
 void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
-                           int64_t* iters, double* relres_out, const double* guess_ref) {
+                           int64_t* iters, double* relres_out, const double* guess_ref, const double* rhs_ref) {
   if (!(tol > 0.0) || max_iter <= 0 || restart <= 0) throw Error(O2F_ERR_ARG, "invalid solver settings");
   const bool full = full_jac();
   if (full) build_full_jacobian();  // first: it recomputes the interface states
   build_jt_blocks();                // (the preconditioner's blocks in the full mode)
-  adjoint_rhs(beta, nullptr);
+  if (rhs_ref) {  // a given right-hand side instead of dJ/dU
+    if (!b_) b_ = arena_.alloc<Vec4<double>>(topo_.nc);
+    to_internal(rhs_ref, b_);
+  } else {
+    adjoint_rhs(beta, nullptr);
+  }
   const int64_t nc = topo_.nc, n4 = 4 * nc;
   auto need = [&](Vec4<double>*& p) {
     if (!p) p = arena_.alloc<Vec4<double>>(nc);

@@ -77,7 +77,8 @@ class Solver {
   void jt_apply(const double* x_ref, double* y_ref);
   void adjoint_rhs(double beta, double* b_ref);
   void adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
-                     int64_t* iters, double* relres, const double* guess_ref = nullptr);
+                     int64_t* iters, double* relres, const double* guess_ref = nullptr,
+                     const double* rhs_ref = nullptr);
   void shape_gradient(const o2f_shape_params& sp, const int* ids, int n, double beta, double eps,
                       const double* lambda_ref, double* grad);
   void debug_perturbed(const o2f_shape_params& sp, int id, double eps, const std::string& which, double* out);
@@ -99,8 +100,10 @@ class Solver {
   void upload_mesh();
   void upload_geometry();
   void compute_phys();
+  // alpha_mode 1 / 2: record / hold the limiter values in fjac_alpha_
+  // (the frozen-limiter linearisation); 0 everywhere else.
   void launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<double>* U, const int* gate,
-                       bool write_grad, const void* rk);
+                       bool write_grad, const void* rk, int alpha_mode = 0);
   void build_jt_blocks();
   // Both linearisations (first-order blocks, full Jacobian) belong to the
   // state, geometry and parameters they were built for.
@@ -109,7 +112,7 @@ class Solver {
     fjac_valid_ = false;
   }
   // consistent adjoint (jacobian.cuh)
-  bool full_jac() const { return params_.adjoint_jacobian == O2F_JAC_FULL; }
+  bool full_jac() const { return params_.adjoint_jacobian != O2F_JAC_REFERENCE; }
   void setup_full_jacobian();
   void build_full_jacobian();
   void jt_apply_dev(const Vec4<double>* x, Vec4<double>* y);
@@ -189,7 +192,7 @@ class Solver {
   std::vector<int64_t> fjac_coff_h_;
   double *fjac_blk_ = nullptr, *fjac_gL_ = nullptr, *fjac_gD_ = nullptr;
   double *fjac_tlp_ = nullptr, *fjac_tdp_ = nullptr, *fjac_tlm_ = nullptr, *fjac_tdm_ = nullptr;
-  Vec4<double>*fjac_Up_ = nullptr, *fjac_Rp_ = nullptr;
+  Vec4<double>*fjac_Up_ = nullptr, *fjac_Rp_ = nullptr, *fjac_alpha_ = nullptr;
   // mesh deformation
   bool deform_alloc_ = false;
   int64_t n_idw_src_ = 0;

@@ -82,7 +82,8 @@ class SimulationParams:
         p.precision = {"fp64": _lib.PREC_F64, "fp32": _lib.PREC_F32}[self.precision.lower()]
         p.adjoint_precond = {"none": 0, "identity": 0, "ilu0": 1}[self.adjoint_precond.lower()]
         p.dt_mode = {"reference": 0, "thermal": 1}[self.dt_mode.lower()]
-        p.adjoint_jacobian = {"reference": 0, "first_order": 0, "full": 1}[self.adjoint_jacobian.lower()]
+        p.adjoint_jacobian = {"reference": 0, "first_order": 0, "full": 1,
+                              "frozen_limiter": 2}[self.adjoint_jacobian.lower()]
         p.verbosity = int(self.verbosity)
         return p
 
@@ -453,6 +454,23 @@ class Solver:
                 raise ValueError("guess must hold 4 values per cell")
             code = lib().o2f_adjoint_solve_guess(self._h, float(beta), float(tol), int(max_iter), int(restart),
                                                  _ptr(g), _ptr(lam), C.byref(it), C.byref(rr))
+        res = {"lambda": lam, "iters": it.value, "relres": rr.value, "status": _lib.STATUS.get(code, "OK")}
+        if code != 0 and raise_on_failure:
+            check(code)
+        return res
+
+    def solve_adjoint_rhs(self, rhs: np.ndarray, tol: float = 1e-6, max_iter: int = 100000, restart: int = 500,
+                          guess: np.ndarray | None = None, raise_on_failure: bool = True) -> dict:
+        """J^T lambda = rhs with the context's operator (o2f_adjoint_solve_rhs)."""
+        b = np.ascontiguousarray(rhs, dtype=np.float64).reshape(-1)
+        if b.size != 4 * self.n_cells:
+            raise ValueError("rhs must hold 4 values per cell")
+        g = None if guess is None else np.ascontiguousarray(guess, dtype=np.float64).reshape(-1)
+        lam = np.empty(4 * self.n_cells)
+        it = C.c_int64()
+        rr = C.c_double()
+        code = lib().o2f_adjoint_solve_rhs(self._h, _ptr(b), float(tol), int(max_iter), int(restart),
+                                           None if g is None else _ptr(g), _ptr(lam), C.byref(it), C.byref(rr))
         res = {"lambda": lam, "iters": it.value, "relres": rr.value, "status": _lib.STATUS.get(code, "OK")}
         if code != 0 and raise_on_failure:
             check(code)

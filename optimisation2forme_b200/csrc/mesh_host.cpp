@@ -13,6 +13,9 @@
 #include "mesh_host.hpp"
 
 #include <algorithm>
+#include <tuple>
+#include <iterator>
+#include <charconv>
 #include <cstring>
 #include <cmath>
 #include <fstream>
@@ -481,43 +484,51 @@ o2f_mesh_desc MshData::desc() const {
   return d;
 }
 
-MshData read_msh2(const std::string& path) {
-  // MSH 2.2 ASCII.  Gmsh exposes, for such a file: nodes in tag order,
-  // physical groups in (dim, tag) order, their elementary entities in
-  // ascending order, and per entity the element types in ascending order with
-  // the elements of a type in file order.  Mesh::Mesh walks exactly that
-  // (src/mesh.cpp:20-179): lines of groups named Inlet/Outlet/FreeStream/
-  // Wall/Airfoil give boundary codes, triangles and quads give cells.
+namespace {
+
+// One msh file's content as read, before the element walk.
+struct MshElem {
+  int type, phys, entity;
+  int64_t n[4];
+};
+struct MshRaw {
+  std::vector<std::tuple<int64_t, double, double>> nodes;  // (tag, x, y), file order
+  std::map<std::pair<int, int>, std::string> names;
+  std::vector<MshElem> elems;
+  bool have_format = false;
+};
+
+int msh_nodes_of(int type) { return type == 1 ? 2 : type == 2 ? 3 : type == 3 ? 4 : type == 15 ? 1 : -1; }
+
+void msh_names(std::istream& in, MshRaw& raw) {
+  int n = 0;
+  in >> n;
+  for (int i = 0; i < n; ++i) {
+    int dim, tag;
+    std::string name;
+    in >> dim >> tag;
+    std::getline(in, name);
+    auto a = name.find('"'), b = name.rfind('"');
+    if (a != std::string::npos && b > a) name = name.substr(a + 1, b - a - 1);
+    raw.names[{dim, tag}] = name;
+  }
+}
+
+// The stream reader: any layout istream accepts.
+MshRaw parse_msh2_stream(const std::string& path) {
   std::ifstream in(path);
   if (!in) throw std::ios_base::failure("cannot open " + path);
-  struct Elem {
-    int type, phys, entity;
-    int64_t n[4];
-  };
-  std::map<int64_t, std::pair<double, double>> nodes;
-  std::map<std::pair<int, int>, std::string> names;
-  std::vector<Elem> elems;
+  MshRaw raw;
   std::string line;
-  bool have_format = false;
   while (std::getline(in, line)) {
     if (line.rfind("$MeshFormat", 0) == 0) {
       double ver;
       int ft, ds;
       in >> ver >> ft >> ds;
       if (ver < 2.0 || ver >= 3.0 || ft != 0) throw std::ios_base::failure("only ASCII MSH 2.x is supported");
-      have_format = true;
+      raw.have_format = true;
     } else if (line.rfind("$PhysicalNames", 0) == 0) {
-      int n = 0;
-      in >> n;
-      for (int i = 0; i < n; ++i) {
-        int dim, tag;
-        std::string name;
-        in >> dim >> tag;
-        std::getline(in, name);
-        auto a = name.find('"'), b = name.rfind('"');
-        if (a != std::string::npos && b > a) name = name.substr(a + 1, b - a - 1);
-        names[{dim, tag}] = name;
-      }
+      msh_names(in, raw);
     } else if (line.rfind("$Nodes", 0) == 0) {
       int64_t n = 0;
       in >> n;
@@ -525,44 +536,203 @@ MshData read_msh2(const std::string& path) {
         int64_t tag;
         double x, y, z;
         in >> tag >> x >> y >> z;
-        nodes[tag] = {x, y};
+        raw.nodes.emplace_back(tag, x, y);
       }
     } else if (line.rfind("$Elements", 0) == 0) {
       int64_t n = 0;
       in >> n;
-      elems.reserve(n);
+      raw.elems.reserve(n);
       for (int64_t i = 0; i < n; ++i) {
         int64_t id;
         int type, ntags;
         in >> id >> type >> ntags;
-        Elem e{type, 0, 0, {0, 0, 0, 0}};
+        MshElem e{type, 0, 0, {0, 0, 0, 0}};
         for (int k = 0; k < ntags; ++k) {
           int t;
           in >> t;
           if (k == 0) e.phys = t;
           if (k == 1) e.entity = t;
         }
-        int nn = type == 1 ? 2 : type == 2 ? 3 : type == 3 ? 4 : type == 15 ? 1 : -1;
+        const int nn = msh_nodes_of(type);
         if (nn < 0) throw std::ios_base::failure("unsupported element type " + std::to_string(type));
         for (int k = 0; k < nn; ++k) in >> e.n[k];
-        elems.push_back(e);
+        raw.elems.push_back(e);
       }
     }
     if (!in && !in.eof()) throw std::ios_base::failure("parse error in " + path);
   }
-  if (!have_format) throw std::ios_base::failure("missing $MeshFormat in " + path);
+  return raw;
+}
+
+// Field scanner for the parallel reader: numbers separated by spaces, tabs
+// or a carriage return; std::from_chars rounds decimal input exactly as the
+// stream does (correct rounding).
+struct Scan {
+  const char* p;
+  const char* e;
+  void skip() {
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+  }
+  template <typename X>
+  bool num(X& v) {
+    skip();
+    if (p < e && *p == '+') ++p;
+    const auto r = std::from_chars(p, e, v);
+    if (r.ec != std::errc() || r.ptr == p) return false;
+    p = r.ptr;
+    return true;
+  }
+  bool at_end() {
+    skip();
+    return p == e;
+  }
+};
+
+// Line starts of [b, e): every line ends with '\n'.
+bool split_lines(const char* b, const char* e, int64_t n, std::vector<const char*>& starts) {
+  if (n < 0) return false;
+  starts.clear();
+  starts.reserve(n + 1);
+  const char* p = b;
+  for (int64_t i = 0; i < n; ++i) {
+    if (p >= e) return false;
+    starts.push_back(p);
+    const char* q = static_cast<const char*>(std::memchr(p, '\n', e - p));
+    if (!q) return false;
+    p = q + 1;
+  }
+  starts.push_back(p);
+  return true;
+}
+
+// The whole file in memory, node and element lines parsed by all threads.
+// Returns false for anything outside the plain layout (one section of each
+// kind, one entry per line), which the stream reader then handles.
+bool parse_msh2_parallel(const std::string& path, MshRaw& raw) {
+  std::ifstream in(path, std::ios::binary | std::ios::ate);
+  if (!in) return false;
+  std::string buf((size_t)in.tellg(), '\0');
+  in.seekg(0);
+  if (!in.read(&buf[0], (std::streamsize)buf.size())) return false;
+  auto section = [&](const char* tag) -> int64_t {  // position after the header line, -1 if absent or repeated
+    const std::string key = std::string("\n") + tag;
+    size_t pos = buf.rfind(tag, 0) == 0 ? 0 : buf.find(key);
+    if (pos == std::string::npos) return -1;
+    if (pos != 0) ++pos;
+    if (buf.find(key, pos + 1) != std::string::npos) return -2;
+    const size_t nl = buf.find('\n', pos);
+    return nl == std::string::npos ? -1 : (int64_t)nl + 1;
+  };
+  const int64_t fmt = section("$MeshFormat"), nam = section("$PhysicalNames"), nod = section("$Nodes"),
+                ele = section("$Elements");
+  if (fmt < 0 || nod < 0 || ele < 0 || nam == -2) return false;
+  {
+    std::istringstream f(buf.substr(fmt, 64));
+    double ver;
+    int ft, ds;
+    if (!(f >> ver >> ft >> ds) || ver < 2.0 || ver >= 3.0 || ft != 0) return false;
+    raw.have_format = true;
+  }
+  if (nam >= 0) {
+    std::istringstream f(buf.substr(nam, buf.find("$EndPhysicalNames", nam) - nam));
+    msh_names(f, raw);
+    if (!f && !f.eof()) return false;
+  }
+  const char* base = buf.data();
+  const char* end = base + buf.size();
+  std::vector<const char*> starts;
+  // $Nodes
+  {
+    Scan h{base + nod, end};
+    int64_t n = 0;
+    if (!h.num(n)) return false;
+    const char* first = static_cast<const char*>(std::memchr(h.p, '\n', end - h.p));
+    if (!first || !split_lines(first + 1, end, n, starts)) return false;
+    raw.nodes.resize(n);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t i = 0; i < n; ++i) {
+      Scan sc{starts[i], starts[i + 1] - 1};
+      int64_t tag;
+      double x, y, z;
+      if (!sc.num(tag) || !sc.num(x) || !sc.num(y) || !sc.num(z) || !sc.at_end()) bad = 1;
+      else raw.nodes[i] = {tag, x, y};
+    }
+    if (bad) return false;
+  }
+  // $Elements
+  {
+    Scan h{base + ele, end};
+    int64_t n = 0;
+    if (!h.num(n)) return false;
+    const char* first = static_cast<const char*>(std::memchr(h.p, '\n', end - h.p));
+    if (!first || !split_lines(first + 1, end, n, starts)) return false;
+    raw.elems.resize(n);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t i = 0; i < n; ++i) {
+      Scan sc{starts[i], starts[i + 1] - 1};
+      int64_t id;
+      int type, ntags;
+      MshElem el{0, 0, 0, {0, 0, 0, 0}};
+      bool ok = sc.num(id) && sc.num(type) && sc.num(ntags) && ntags >= 0;
+      for (int k = 0; ok && k < ntags; ++k) {
+        int t;
+        ok = sc.num(t);
+        if (k == 0) el.phys = t;
+        if (k == 1) el.entity = t;
+      }
+      const int nn = msh_nodes_of(type);
+      ok = ok && nn > 0;
+      for (int k = 0; ok && k < nn; ++k) ok = sc.num(el.n[k]);
+      el.type = type;
+      if (!ok || !sc.at_end()) bad = 1;
+      else raw.elems[i] = el;
+    }
+    if (bad) return false;
+  }
+  return true;
+}
+
+// Gmsh exposes, for an MSH 2.2 file: nodes in tag order (a repeated tag
+// keeps its last line), physical groups in (dim, tag) order, their
+// elementary entities in ascending order, and per entity the element types
+// in ascending order with the elements of a type in file order.  Mesh::Mesh
+// walks exactly that (src/mesh.cpp:20-179): lines of groups named
+// Inlet/Outlet/FreeStream/Wall/Airfoil give boundary codes, triangles and
+// quads give cells.
+MshData assemble_msh(const std::string& path, MshRaw& raw) {
+  if (!raw.have_format) throw std::ios_base::failure("missing $MeshFormat in " + path);
   MshData out;
-  std::map<int64_t, int64_t> vmap;
-  for (const auto& [tag, xy] : nodes) {
-    vmap[tag] = (int64_t)out.xy.size() / 2;
-    out.xy.push_back(xy.first);
-    out.xy.push_back(xy.second);
+  auto& nodes = raw.nodes;
+  std::stable_sort(nodes.begin(), nodes.end(),
+                   [](const auto& a, const auto& b) { return std::get<0>(a) < std::get<0>(b); });
+  std::vector<int64_t> tags;
+  tags.reserve(nodes.size());
+  for (size_t i = 0; i < nodes.size(); ++i) {
+    if (i + 1 < nodes.size() && std::get<0>(nodes[i + 1]) == std::get<0>(nodes[i])) continue;  // last one wins
+    tags.push_back(std::get<0>(nodes[i]));
+    out.xy.push_back(std::get<1>(nodes[i]));
+    out.xy.push_back(std::get<2>(nodes[i]));
+  }
+  // tag -> vertex: a table when the tags are about dense (Gmsh numbers them
+  // 1..N), else a binary search
+  std::vector<int64_t> lut;
+  if (!tags.empty() && tags.front() >= 0 && tags.back() <= 4 * (int64_t)tags.size() + 16) {
+    lut.assign(tags.back() + 1, -1);
+    for (size_t i = 0; i < tags.size(); ++i) lut[tags[i]] = (int64_t)i;
   }
   auto vid = [&](int64_t tag) {
-    auto it = vmap.find(tag);
-    if (it == vmap.end()) throw std::ios_base::failure("element references unknown node " + std::to_string(tag));
-    return it->second;
+    if (!lut.empty()) {
+      if (tag >= 0 && tag < (int64_t)lut.size() && lut[tag] >= 0) return lut[tag];
+      throw std::ios_base::failure("element references unknown node " + std::to_string(tag));
+    }
+    auto it = std::lower_bound(tags.begin(), tags.end(), tag);
+    if (it == tags.end() || *it != tag)
+      throw std::ios_base::failure("element references unknown node " + std::to_string(tag));
+    return (int64_t)(it - tags.begin());
   };
+  const auto& elems = raw.elems;
   auto dim_of = [](int type) { return type == 15 ? 0 : type == 1 ? 1 : 2; };
   std::set<std::pair<int, int>> groups;
   for (const auto& e : elems)
@@ -570,8 +740,8 @@ MshData read_msh2(const std::string& path) {
   out.coff.push_back(0);
   for (const auto& [dim, tag] : groups) {
     std::string name;
-    auto itn = names.find({dim, tag});
-    if (itn != names.end()) name = itn->second;
+    auto itn = raw.names.find({dim, tag});
+    if (itn != raw.names.end()) name = itn->second;
     uint8_t code = name == "Inlet" ? 'i'
                  : name == "Outlet" ? 'o'
                  : name == "FreeStream" ? 'f'
@@ -600,6 +770,20 @@ MshData read_msh2(const std::string& path) {
     }
   }
   return out;
+}
+
+}  // namespace
+
+MshData read_msh2(const std::string& path) {
+  constexpr std::streamoff kParallelFrom = 1 << 20;  // bytes; smaller files take the stream reader
+  MshRaw raw;
+  {
+    std::ifstream probe(path, std::ios::binary | std::ios::ate);
+    if (!probe) throw std::ios_base::failure("cannot open " + path);
+    if (probe.tellg() >= kParallelFrom && parse_msh2_parallel(path, raw)) return assemble_msh(path, raw);
+  }
+  raw = parse_msh2_stream(path);
+  return assemble_msh(path, raw);
 }
 
 }  // namespace o2f

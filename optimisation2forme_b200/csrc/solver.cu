@@ -503,10 +503,18 @@ void Solver::render_field(const std::string& field, int nx, int ny, const std::s
   const double span = fmax_ - fmin_;
   std::memset(rgb, 0, 3 * (size_t)npix);
   if (!(span > 0.0)) return;  // render_scalar_field_unstructured draws nothing
-  unsigned long long* pix = nullptr;
-  unsigned char* img = nullptr;
-  O2F_CUDA(cudaMallocAsync(&pix, npix * sizeof(unsigned long long), s));
-  O2F_CUDA(cudaMallocAsync(&img, 3 * npix, s));
+  // per-call scratch (the image size varies), freed on every exit
+  struct Scratch {
+    void* p = nullptr;
+    cudaStream_t s;
+    ~Scratch() {
+      if (p) cudaFreeAsync(p, s);
+    }
+  } pix_buf{nullptr, s}, img_buf{nullptr, s};
+  O2F_CUDA(cudaMallocAsync(&pix_buf.p, npix * sizeof(unsigned long long), s));
+  O2F_CUDA(cudaMallocAsync(&img_buf.p, 3 * npix, s));
+  auto* pix = static_cast<unsigned long long*>(pix_buf.p);
+  auto* img = static_cast<unsigned char*>(img_buf.p);
   RenderView w{x_min, y_min, std::abs(x_max - x_min), std::abs(y_max - y_min), nx, ny};
   O2F_CUDA(cudaMemsetAsync(pix, 0xff, npix * sizeof(unsigned long long), s));
   k_raster_cells<<<grid(nc), kBlock, 0, s>>>(nc, topo_.cverts, topo_.ctype, geom_.vxy, render_ref_id_, w, pix);
@@ -514,8 +522,6 @@ void Solver::render_field(const std::string& field, int nx, int ny, const std::s
                                                                          cmap == "schlieren" ? 1 : 0, img);
   O2F_CUDA(cudaGetLastError());
   O2F_CUDA(cudaMemcpyAsync(rgb, img, 3 * npix, cudaMemcpyDeviceToHost, s));
-  O2F_CUDA(cudaFreeAsync(pix, s));
-  O2F_CUDA(cudaFreeAsync(img, s));
   sync();
   launches_ += 4;
 }

@@ -245,13 +245,13 @@ HostMesh build_mesh_gpu(const o2f_mesh_desc& d, void* stream_ptr) {
     check_cuda(cudaMemcpyAsync(&e, err.p, sizeof(e), cudaMemcpyDeviceToHost, s), "copy");
     check_cuda(cudaStreamSynchronize(s), "topology build");
     if (e == ~0ull) return;
+    // the host build's messages (the index of the first fault is in the low
+    // 48 bits, which those messages do not carry)
     const int kind = (int)(e >> 48);
-    const int64_t i = (int64_t)(e & ((1ull << 48) - 1));
     static const char* msg[] = {"only triangles and quadrilaterals are supported", "cell vertex out of range",
                                 "edge shared by more than two cells", "boundary edge without a boundary condition",
                                 "interior edge carries a boundary condition", "cell with a repeated vertex",
                                 "vertex valence above the GPU build's limit"};
-    (void)i;
     if (kind == kErrValence) throw TopologyLimit(O2F_ERR_MESH, msg[kind]);
     throw Error(O2F_ERR_MESH, msg[kind]);
   };

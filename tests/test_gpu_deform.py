@@ -66,6 +66,15 @@ def test_deformation_moves_the_wall_by_the_perturbation_formula():
         dwall = np.linalg.norm(xy1[wall] - xy0[wall], axis=1).max()
         dint = np.linalg.norm(xy1[vbc == 0] - xy0[vbc == 0], axis=1)
         assert dwall > 0 and 0 < dint.max() <= dwall * (1 + 1e-12)
+        # the interior against inverse distance weighting restated in numpy:
+        # all boundary vertices are sources, weights |r|^-4
+        src = vbc != 0
+        d_src = np.where(wall[src][:, None], wall_ref[src] - xy0[src], 0.0)
+        inner = np.nonzero(vbc == 0)[0]
+        r2 = ((xy0[inner][:, None, :] - xy0[src][None, :, :]) ** 2).sum(-1)
+        w = 1.0 / (r2 * r2)
+        want = xy0[inner] + (w @ d_src) / w.sum(axis=1)[:, None]
+        assert np.abs(xy1[inner] - want).max() <= 1e-12 * dwall
         # the context's geometry is the host build on the moved coordinates
         h = HostMesh(desc=desc_of(dict(a, node_xy=xy1.reshape(-1))))
         for name in ("cell_vol", "edge_n", "vert_w"):

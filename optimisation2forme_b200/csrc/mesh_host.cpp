@@ -364,6 +364,72 @@ void compute_vertex_weights(HostMesh& m) {
   }  // omp parallel
 }
 
+Stencil jacobian_stencil(const HostMesh& m, const std::vector<int64_t>& perm, const std::vector<int64_t>& cinv) {
+  const int64_t nc = m.nc;
+  // ring(c): cells sharing a vertex with c, ascending (new numbering)
+  std::vector<int64_t> roff(nc + 1, 0);
+  std::vector<std::vector<int32_t>> ring(nc);
+#pragma omp parallel
+  {
+    std::vector<int32_t> tmp;
+#pragma omp for schedule(static)
+    for (int64_t c = 0; c < nc; ++c) {
+      const int64_t co = perm[c];
+      tmp.clear();
+      for (int64_t k = m.cell_voff[co]; k < m.cell_voff[co + 1]; ++k) {
+        const int64_t v = m.cell_verts[k];
+        for (int64_t q = m.vert_coff[v]; q < m.vert_coff[v + 1]; ++q) tmp.push_back((int32_t)cinv[m.vert_cells[q]]);
+      }
+      std::sort(tmp.begin(), tmp.end());
+      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+      ring[c] = tmp;
+    }
+  }
+  // S(c) = ring(ring(c))
+  Stencil st;
+  std::vector<std::vector<int32_t>> sten(nc);
+#pragma omp parallel
+  {
+    std::vector<int32_t> tmp;
+#pragma omp for schedule(static)
+    for (int64_t c = 0; c < nc; ++c) {
+      tmp.clear();
+      for (int32_t a : ring[c]) tmp.insert(tmp.end(), ring[a].begin(), ring[a].end());
+      std::sort(tmp.begin(), tmp.end());
+      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+      sten[c] = tmp;
+    }
+  }
+  std::vector<std::vector<int32_t>>().swap(ring);
+  st.off.assign(nc + 1, 0);
+  for (int64_t c = 0; c < nc; ++c) st.off[c + 1] = st.off[c] + (int64_t)sten[c].size();
+  st.idx.resize(st.off[nc]);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) std::copy(sten[c].begin(), sten[c].end(), st.idx.begin() + st.off[c]);
+  std::vector<std::vector<int32_t>>().swap(sten);
+  // greedy colouring in new order: the colours of every cell sharing some
+  // S(i) with j are taken
+  st.color.assign(nc, -1);
+  std::vector<int64_t> mark;
+  for (int64_t j = 0; j < nc; ++j) {
+    for (int64_t a = st.off[j]; a < st.off[j + 1]; ++a) {
+      const int32_t i = st.idx[a];
+      for (int64_t b = st.off[i]; b < st.off[i + 1]; ++b) {
+        const int32_t col = st.color[st.idx[b]];
+        if (col >= 0) mark[col] = j;
+      }
+    }
+    int32_t col = 0;
+    while (col < st.ncolor && mark[col] == j) ++col;
+    if (col == st.ncolor) {
+      ++st.ncolor;
+      mark.push_back(-1);
+    }
+    st.color[j] = col;
+  }
+  return st;
+}
+
 double min_cell_h(const HostMesh& m) {
   double min_h = INFINITY;
   for (int64_t c = 0; c < m.nc; ++c) {

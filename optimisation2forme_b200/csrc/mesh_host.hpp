@@ -89,6 +89,19 @@ double min_cell_h(const HostMesh& m);
 // its length.  Throws std::invalid_argument for an unknown name.
 int64_t export_mesh_array(const HostMesh& m, const std::string& which, void* out);
 
+// Stencil of the full residual Jacobian: for every cell c (numbered by
+// cinv: new = cinv[old], perm the inverse), the cells within two vertex
+// rings, S(c), as an ascending CSR in the new numbering (the relation is
+// symmetric); and a greedy colouring of the cells in new order such that no
+// S(i) holds two cells of one colour.
+struct Stencil {
+  std::vector<int64_t> off;
+  std::vector<int32_t> idx;
+  std::vector<int32_t> color;
+  int32_t ncolor = 0;
+};
+Stencil jacobian_stencil(const HostMesh& m, const std::vector<int64_t>& perm, const std::vector<int64_t>& cinv);
+
 // Hilbert-curve order of points (x, y): returns perm with perm[new] = old.
 std::vector<int64_t> hilbert_order(const std::vector<double>& x, const std::vector<double>& y);
 

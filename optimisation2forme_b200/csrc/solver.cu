@@ -1067,66 +1067,11 @@ void Solver::setup_full_jacobian() {
   if (fjac_setup_) return;
   const HostMesh& m = hm_;
   const int64_t nc = m.nc;
-  // cells sharing a vertex with cell c (device numbering, ascending)
-  std::vector<int64_t> voff(nc + 1, 0);
-  std::vector<int32_t> vcl;
-  std::vector<int64_t> stamp(nc, -1);
-  std::vector<int32_t> tmp;
-  for (int64_t c = 0; c < nc; ++c) {
-    const int64_t co = cperm_[c];
-    tmp.clear();
-    for (int64_t k = m.cell_voff[co]; k < m.cell_voff[co + 1]; ++k) {
-      const int64_t v = m.cell_verts[k];
-      for (int64_t q = m.vert_coff[v]; q < m.vert_coff[v + 1]; ++q) {
-        const int64_t c2 = cinv_[m.vert_cells[q]];
-        if (stamp[c2] != c) {
-          stamp[c2] = c;
-          tmp.push_back((int32_t)c2);
-        }
-      }
-    }
-    std::sort(tmp.begin(), tmp.end());
-    vcl.insert(vcl.end(), tmp.begin(), tmp.end());
-    voff[c + 1] = (int64_t)vcl.size();
-  }
-  // S(c): two rings
-  std::fill(stamp.begin(), stamp.end(), -1);
-  std::vector<int64_t> soff(nc + 1, 0);
-  std::vector<int32_t> sidx;
-  for (int64_t c = 0; c < nc; ++c) {
-    tmp.clear();
-    for (int64_t a = voff[c]; a < voff[c + 1]; ++a)
-      for (int64_t b = voff[vcl[a]]; b < voff[vcl[a] + 1]; ++b) {
-        const int32_t c2 = vcl[b];
-        if (stamp[c2] != c) {
-          stamp[c2] = c;
-          tmp.push_back(c2);
-        }
-      }
-    std::sort(tmp.begin(), tmp.end());
-    sidx.insert(sidx.end(), tmp.begin(), tmp.end());
-    soff[c + 1] = (int64_t)sidx.size();
-  }
-  // greedy colouring: no two cells of one colour in any S(i)
-  std::vector<int32_t> color(nc, -1);
-  std::vector<int64_t> mark;
-  int32_t ncol = 0;
-  for (int64_t j = 0; j < nc; ++j) {
-    for (int64_t a = soff[j]; a < soff[j + 1]; ++a) {
-      const int32_t i = sidx[a];
-      for (int64_t b = soff[i]; b < soff[i + 1]; ++b) {
-        const int32_t col = color[sidx[b]];
-        if (col >= 0) mark[col] = j;
-      }
-    }
-    int32_t col = 0;
-    while (col < ncol && mark[col] == j) ++col;
-    if (col == ncol) {
-      ++ncol;
-      mark.push_back(-1);
-    }
-    color[j] = col;
-  }
+  Stencil stc = jacobian_stencil(m, cperm_, cinv_);
+  const std::vector<int64_t>& soff = stc.off;
+  const std::vector<int32_t>& sidx = stc.idx;
+  const std::vector<int32_t>& color = stc.color;
+  const int32_t ncol = stc.ncolor;
   fjac_coff_h_.assign(ncol + 1, 0);
   for (int64_t j = 0; j < nc; ++j) ++fjac_coff_h_[color[j] + 1];
   for (int32_t c = 0; c < ncol; ++c) fjac_coff_h_[c + 1] += fjac_coff_h_[c];

@@ -79,3 +79,30 @@ def test_msh_reader_errors(tmp_path):
     with pytest.raises(O2FError) as e:
         HostMesh(f)
     assert e.value.status == "O2F_ERR_IO"
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """Every struct of include/o2f.h has the size and field offsets that the
+    ctypes mirror in _lib.py uses (a C program compiled here prints them)."""
+    import shutil
+    from optimisation2forme_b200 import _lib
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc is needed")
+    mirrors = {"o2f_params": _lib.Params, "o2f_mesh_desc": _lib.MeshDesc, "o2f_shape_params": _lib.ShapeParams,
+               "o2f_mesh_info": _lib.MeshInfo, "o2f_timing": _lib.Timing}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "o2f.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    for line in filter(None, out):
+        cname, field, value = line.split()
+        cls = mirrors[cname]
+        want = C.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        assert int(value) == want, line

@@ -167,7 +167,10 @@ const char* o2f_version(void);
 /* Host-only mesh build (no GPU needed): the topology, geometry and
  * interpolation weights the context is built from, in reference order.  The
  * construction replaces navier_stokes::Mesh::Mesh (src/mesh.cpp:7-283) and
- * recordEdge (:288-297).  Export names: see o2f_mesh_export. */
+ * recordEdge (:288-297).  Export names: see o2f_mesh_export.  .msh files
+ * (ASCII MSH 2.x) from 1 MB have their node and element lines parsed by all
+ * host threads, with the result of the stream parser used below that size
+ * and for irregular layouts. */
 int o2f_host_mesh_create(const o2f_mesh_desc* mesh, o2f_host_mesh** out);
 int o2f_host_mesh_from_msh(const char* path, o2f_host_mesh** out);
 

@@ -208,6 +208,7 @@ void Batch::tune(int reps, int* cfg_out) {
 }
 
 void Batch::rk3_run(int64_t max_steps, double drop_tol, int64_t* steps_done, double* t_out, int* status) {
+  NvtxRange nvtx_("o2f batch_rk3_run");
   if (max_steps < 0) throw Error(O2F_ERR_ARG, "max_steps < 0");
   const int n = (int)s_.size();
   if (hist_cap_ < std::max<int64_t>(max_steps, 1)) {

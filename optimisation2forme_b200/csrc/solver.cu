@@ -376,6 +376,7 @@ void Solver::upload_geometry() {
 }
 
 void Solver::set_vertex_coords(const double* xy) {
+  NvtxRange nvtx_("o2f set_vertex_coords");
   try {
     set_coordinates(hm_, xy);
   } catch (const std::invalid_argument& e) {
@@ -391,6 +392,7 @@ void Solver::set_vertex_coords(const double* xy) {
 }
 
 void Solver::deform_shape(const o2f_shape_params& from, const o2f_shape_params& to, int power) {
+  NvtxRange nvtx_("o2f deform_shape");
   if (power < 1 || power > 8) throw Error(O2F_ERR_ARG, "IDW power must be in [1, 8]");
   if (from.pos_x != to.pos_x || from.c != to.c)
     throw Error(O2F_ERR_ARG, "deform_shape moves m, p, t; pos_x and c must not change");
@@ -443,6 +445,7 @@ void Solver::deform_shape(const o2f_shape_params& from, const o2f_shape_params& 
 
 void Solver::render_field(const std::string& field, int nx, int ny, const std::string& cmap, const double* range_in,
                           unsigned char* rgb, double* range_out) {
+  NvtxRange nvtx_("o2f render_field");
   static const char* names[] = {"rho", "rho_u", "rho_v", "E", "u", "v", "u_x", "u_y", "v_x", "v_y", "div", "p"};
   int f = -1;
   for (int k = 0; k < 12; ++k)
@@ -624,6 +627,7 @@ void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector
 }
 
 void Solver::ilu_factor() {
+  NvtxRange nvtx_("o2f ilu_factor");
   const int64_t nc = topo_.nc;
   cudaStream_t s = stream_;
   if (!ilu_alloc_) {
@@ -807,6 +811,7 @@ void Solver::launch_residual(const Geom<double>& g, const Work<double>& w, Vec4<
 }
 
 void Solver::residual(double* R_ref) {
+  NvtxRange nvtx_("o2f residual");
   if (f32()) {
     ensure_f32();
     f32_state_sync();
@@ -938,6 +943,7 @@ void Solver::debug_get(const std::string& which, double* out) {
 }
 
 void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_t* steps_done, double* t_out) {
+  NvtxRange nvtx_("o2f rk3_run");
   if (max_steps < 0) throw Error(O2F_ERR_ARG, "max_steps < 0");
   if (hist_cap_ < std::max<int64_t>(max_steps, 1)) {
     hist_cap_ = std::max<int64_t>(max_steps, 1);
@@ -1043,6 +1049,7 @@ void Solver::forces(double beta, double* out3) {
 }
 
 void Solver::build_jt_blocks() {
+  NvtxRange nvtx_("o2f jt_blocks");
   if (blk_valid_) return;
   if (!have_residual_) throw Error(O2F_ERR_STATE, "no residual has been evaluated");
   if (!blk_) blk_ = arena_.alloc<double>(32 * topo_.ne);
@@ -1064,6 +1071,7 @@ void Solver::jt_apply_dev(const Vec4<double>* x, Vec4<double>* y) {
 // Stencils (two vertex rings), their colouring, and the wall edges each cell
 // reaches; host work, once per mesh topology.
 void Solver::setup_full_jacobian() {
+  NvtxRange nvtx_("o2f full_jacobian_setup");
   if (fjac_setup_) return;
   const HostMesh& m = hm_;
   const int64_t nc = m.nc;
@@ -1123,6 +1131,7 @@ void Solver::setup_full_jacobian() {
 // then the columns of the blocks and the objective gradient.  Leaves the
 // residual and interface states of the current state in the context.
 void Solver::build_full_jacobian() {
+  NvtxRange nvtx_("o2f full_jacobian");
   if (fjac_valid_) return;
   setup_full_jacobian();
   const int64_t nc = topo_.nc, nw = topo_.n_wall;
@@ -1218,6 +1227,7 @@ void Solver::adjoint_rhs(double beta, double* b_ref) {
 
 void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t restart, double* lambda_ref,
                            int64_t* iters, double* relres_out, const double* guess_ref, const double* rhs_ref) {
+  NvtxRange nvtx_("o2f adjoint_solve");
   if (!(tol > 0.0) || max_iter <= 0 || restart <= 0) throw Error(O2F_ERR_ARG, "invalid solver settings");
   const bool full = full_jac();
   if (full) build_full_jacobian();  // first: it recomputes the interface states
@@ -1441,6 +1451,7 @@ void Solver::perturbed_geometry(const o2f_shape_params& sp, int id, double eps) 
 
 void Solver::shape_gradient(const o2f_shape_params& sp, const int* ids, int n, double beta, double eps,
                             const double* lambda_ref, double* grad) {
+  NvtxRange nvtx_("o2f shape_gradient");
   if (n < 0 || (n > 0 && (!ids || !grad))) throw Error(O2F_ERR_ARG, "invalid parameter list");
   if (!(eps > 0.0)) throw Error(O2F_ERR_ARG, "eps must be positive");
   if (!lam_) lam_ = arena_.alloc<Vec4<double>>(topo_.nc);

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <memory>
 #include <stdexcept>
@@ -17,6 +18,16 @@ namespace o2f {
 
 struct KrylovState;
 struct StepState;
+
+// NVTX range over a host stage (residual, time loop, adjoint, gradient,
+// Jacobian builds, mesh updates, images): named spans for Nsight tools; a
+// no-op when no tool is attached (NVTX v3 is header-only).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct Error : std::runtime_error {
   int code;

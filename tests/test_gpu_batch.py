@@ -115,3 +115,34 @@ def test_candidates_stop_independently():
     finally:
         for s in ctxs:
             s.close()
+
+
+def test_poisoned_candidate_fails_alone():
+    """A non-finite state in one candidate stops that candidate with
+    O2F_ERR_NONFINITE; the others run their steps, bit-identical to their
+    own single-context runs, and the batch stays usable."""
+    from optimisation2forme_b200 import Batch
+    ref = _single_runs(30)
+    ctxs = _contexts()
+    try:
+        for s in ctxs:
+            s.initialize_freestream()
+        U = ctxs[1].get_state()
+        U[4 * 5 + 1] = np.nan
+        ctxs[1].set_state(U)
+        with Batch(ctxs) as b:
+            res = b.time_loop(30)
+            assert res[1]["status"] == "O2F_ERR_NONFINITE" and res[1]["steps"] < 30
+            for i in (0, 2):
+                assert res[i]["status"] == "OK" and res[i]["steps"] == 30
+                assert bits_equal(ctxs[i].get_state(), ref[i][0])
+            # the batch runs again once the candidate has a finite state
+            ctxs[1].initialize_freestream()
+            for i in (0, 2):
+                ctxs[i].initialize_freestream()
+            again = b.time_loop(30)
+            assert all(r["status"] == "OK" and r["steps"] == 30 for r in again)
+            assert bits_equal(ctxs[1].get_state(), ref[1][0])
+    finally:
+        for s in ctxs:
+            s.close()

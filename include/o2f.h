@@ -406,6 +406,15 @@ int o2f_mlp_gradients(o2f_mlp* net, const float* inputs, const float* targets, i
 int o2f_mlp_get_params(o2f_mlp* net, float* params, float* freq);
 int o2f_mlp_set_params(o2f_mlp* net, const float* params);
 
+/* Test hook of the failure path (no counterpart in the reference).  The
+ * block-ILU(0) sweeps wait, bounded, on the ready flags of the rows they
+ * depend on; a wait that runs out makes the solve return O2F_ERR_CUDA and
+ * leaves the context usable.  With stall != 0 the solves started after this
+ * call run with one row that never releases its flag and with spin_limit
+ * polls per wait (<= 0: the default of 2^22), so that path can be exercised
+ * without any GPU fault; stall = 0, spin_limit = 0 restores the defaults. */
+int o2f_debug_ilu_stall(o2f_ctx* ctx, int stall, int64_t spin_limit);
+
 /* No counterpart in the reference.  For callers that may not allocate
  * device memory during a call -- a host time loop calling it every step,
  * where cudaMalloc would synchronise the device, or a host that owns all
@@ -416,7 +425,12 @@ int o2f_mlp_set_params(o2f_mlp* net, const float* params);
  * Limit: meshes of at most 16,777,216 cells (O2F_ERR_ARG beyond).  Calls
  * that overlap on one device share that scratch and race: serialise them.
  * The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress); make it before any stream capture. */
+ * (cudaGetSymbolAddress); make it before any stream capture.  That address
+ * is cached for the life of the process: after a cudaDeviceReset of the
+ * device, do not call this entry point on it again.  In an FP32 context the
+ * residual is o2f_residual's FP32 one (FP64 R, FP64 norm); such a context
+ * needs one o2f_residual or o2f_rk3_run before the first call, which
+ * allocate its FP32 buffers (O2F_ERR_STATE otherwise). */
 int o2f_residual_norm_noalloc(o2f_ctx* ctx, double* norm_out);
 
 /* No counterpart in the reference, whose outer loop (mesh_opti/run_opti.sh)

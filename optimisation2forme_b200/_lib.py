@@ -139,6 +139,7 @@ SIGNATURES = {
     "o2f_get_timing": ([_vp, C.POINTER(Timing)], C.c_int),
     "o2f_profile_kernels": ([_vp, C.c_int, _dp], C.c_int),
     "o2f_residual_norm_noalloc": ([_vp, _dp], C.c_int),
+    "o2f_debug_ilu_stall": ([_vp, C.c_int, C.c_int64], C.c_int),
     "o2f_host_mesh_set_coords": ([_vp, _dp], C.c_int),
     "o2f_checkpoint_write": ([C.c_char_p, C.c_int64, _dp, C.c_double, C.c_int64], C.c_int),
     "o2f_checkpoint_read": ([C.c_char_p, C.c_int64, _dp, _dp, C.POINTER(C.c_int64)], C.c_int),

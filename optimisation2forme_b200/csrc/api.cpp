@@ -509,6 +509,10 @@ int o2f_mlp_set_params(o2f_mlp* net, const float* params) {
   });
 }
 
+int o2f_debug_ilu_stall(o2f_ctx* ctx, int stall, int64_t spin_limit) {
+  return guarded([&] { S(ctx).debug_ilu_stall(stall, (long long)spin_limit); });
+}
+
 int o2f_residual_norm_noalloc(o2f_ctx* ctx, double* norm_out) {
   return guarded([&] {
     need(norm_out, "norm_out");

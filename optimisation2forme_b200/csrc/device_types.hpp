@@ -117,12 +117,15 @@ struct IluDev {
   int32_t* nbr;       // [4*nc] neighbour cell of each slot (slot order = jslot order), -1 if none
   int32_t* pos;       // [nc] position of the cell in the ILU order
   int32_t* order;     // [nc] cell at each ILU position (inverse of pos)
+  int32_t* sweep;     // [2*nc] processing orders of the forward, then the backward sweep
   double* A;          // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
   double* Dinv;       // [nc*16]
   int32_t* lo_cells;  // [nc] factorization levels, concatenated (offsets kept on the host)
   uint32_t* flag;     // [2*nc] ready flags of the forward, then the backward sweep
   SweepSync* sync;    // [2] forward, backward
   int n_lo;
+  long long spin_limit;  // polls a sweep row waits before it gives up (error status)
+  int32_t stall_row;     // test hook: this row never releases its forward flag (-1: none)
 };
 
 // Buffers written by one residual evaluation.

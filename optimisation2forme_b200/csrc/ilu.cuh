@@ -188,13 +188,17 @@ __global__ void __launch_bounds__(128) k_ilu_factor(const int32_t* __restrict__ 
   if (!mat4_inv(row, ilu.Dinv + (int64_t)i * 16)) atomicExch(status, 1);
 }
 
-// Sync-free triangular sweeps (one launch per triangle).  Each warp takes
-// one 32-row chunk of the ILU order from a counter, so every chunk before it
-// already belongs to a running warp and the earliest unfinished row always
-// has its dependencies done: the waits cannot deadlock.  A row waits on the
+// Sync-free triangular sweeps (one launch per triangle).  Rows are processed
+// in a level order of the triangle's dependency graph (ilu.sweep: forward
+// levels, then backward levels), a topological order, so the rows of one
+// 32-row chunk are mostly independent.  Each warp takes one chunk from a
+// counter, so every chunk before it already belongs to a running warp and
+// the earliest unfinished row always has its dependencies done: the waits
+// cannot deadlock.  A row waits on the
 // ready flags of its lower (forward) or upper (backward) neighbours, solves
 // its 4-vector and releases its own flag.  Waits are bounded: past
-// kSweepSpinLimit polls the warp records sync->err and stops waiting, and
+// ilu.spin_limit polls (default kSweepSpinLimit) the warp records sync->err
+// and stops waiting, and
 // every other waiting row gives up once it sees the error.
 constexpr int kSweepBlock = 128;
 constexpr long long kSweepSpinLimit = 1ll << 22;
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
   const bool active = p < n;
   int i = 0, dep[4], ndep = 0, slot[4];
   if (active) {
-    i = ilu.order[kForward ? p : n - 1 - p];
+    i = ilu.sweep[kForward ? p : (int64_t)n + p];
     const int pi = ilu.pos[i];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -284,10 +288,11 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
         acc = out;
       }
       y[i] = acc;
-      st_release_u32(flag + i, want);  // orders the store of y[i] before the flag
+      if (!kForward || i != ilu.stall_row)
+        st_release_u32(flag + i, want);  // orders the store of y[i] before the flag
       done = true;
     } else if ((++spins & 63) == 0) {
-      if (spins > kSweepSpinLimit) {
+      if (spins > ilu.spin_limit) {
         atomicExch(&sync->err, 1);
         done = true;
       } else if (*reinterpret_cast<volatile int*>(&sync->err)) {

@@ -27,7 +27,14 @@
 // Set-up: the scratch address is looked up with cudaGetSymbolAddress once
 // per device, on the first call made with that device current, and cached.
 // That first call therefore does set-up work; make it before any stream
-// capture.
+// capture.  The cached address belongs to the device's context at that
+// time: after a cudaDeviceReset (or any reset of the primary context) it is
+// stale, so a process that resets a device must not call this entry point
+// on that device again.
+//
+// Precision: the residual is the one o2f_residual computes for the context
+// (FP64, or in an FP32 context the FP32 residual with FP64 R); the norm is
+// always reduced in FP64.
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -128,7 +135,21 @@ void Solver::residual_norm_noalloc(double* norm_out) {
     throw Error(O2F_ERR_ARG, "o2f_residual_norm_noalloc: " + std::to_string(nc) +
                                  " cells exceed the static scratch limit of 16777216 cells");
   const NormScratch sc = norm_scratch();
-  launch_residual(geom_, work_, U_, nullptr, true, nullptr);
+  if (f32()) {
+    // As o2f_residual in an FP32 context: FP32 residual, FP64 R and the
+    // widened interface states.  Its buffers come from the context's first
+    // FP32 residual or time loop, which this call may not allocate.
+    if (!f32_ready_)
+      throw Error(O2F_ERR_STATE,
+                  "o2f_residual_norm_noalloc: an FP32 context needs one o2f_residual or o2f_rk3_run first "
+                  "(it allocates the FP32 buffers)");
+    ensure_f32();
+    f32_state_sync();
+    launch_residual_f32(nullptr, nullptr);
+    f32_publish_interfaces();
+  } else {
+    launch_residual(geom_, work_, U_, nullptr, true, nullptr);
+  }
   have_residual_ = true;
   invalidate_linearisation();
   const int blocks = (int)((nc + kNormCellsPerBlock - 1) / kNormCellsPerBlock);

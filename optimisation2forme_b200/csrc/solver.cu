@@ -621,9 +621,39 @@ void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector
     nlo = std::max(nlo, l + 1);
   }
   bucket(nlo, lo_off_h_, lo_cells_h_);
+  // Sweep orders: the forward solve's rows by forward level (the
+  // factorization's level sets above, each in RCM order), the backward
+  // solve's by the levels of the upper-triangle dependencies.  Both are
+  // topological orders of their triangle, so each row computes exactly what
+  // it computes in the RCM order, but the rows a warp claims together no
+  // longer wait on one another.
+  std::vector<int32_t> levu(nc, 0);
+  int nup = 0;
+  for (int64_t i = nc - 1; i >= 0; --i) {
+    const int32_t c = order[i];
+    int l = 0;
+    for (int k = 0; k < 4; ++k) {
+      const int32_t o = nbr(c, k);
+      if (o >= 0 && ilu_pos_h_[o] > i) l = std::max(l, levu[o] + 1);
+    }
+    levu[c] = l;
+    nup = std::max(nup, l + 1);
+  }
+  std::vector<int32_t> up_off(nup + 1, 0);
+  for (int64_t c = 0; c < nc; ++c) up_off[levu[c] + 1]++;
+  for (int l = 0; l < nup; ++l) up_off[l + 1] += up_off[l];
+  ilu_sweep_h_.assign(2 * nc, 0);
+  std::copy(lo_cells_h_.begin(), lo_cells_h_.end(), ilu_sweep_h_.begin());
+  {
+    std::vector<int32_t> fill(up_off.begin(), up_off.end() - 1);
+    for (int64_t i = nc - 1; i >= 0; --i) ilu_sweep_h_[nc + fill[levu[order[i]]]++] = order[i];
+  }
+  ilu_n_up_ = nup;
   ilu_order_h_ = std::move(order);
   ilu_.nc = nc;
   ilu_.n_lo = nlo;
+  ilu_.spin_limit = kSweepSpinLimit;
+  ilu_.stall_row = -1;
 }
 
 void Solver::ilu_factor() {
@@ -636,6 +666,7 @@ void Solver::ilu_factor() {
     ilu_.A = arena_.alloc<double>(80 * nc);
     ilu_.Dinv = arena_.alloc<double>(16 * nc);
     ilu_.order = arena_.alloc<int32_t>(nc);
+    ilu_.sweep = arena_.alloc<int32_t>(2 * nc);
     ilu_.lo_cells = arena_.alloc<int32_t>(nc);
     ilu_.flag = arena_.alloc<uint32_t>(2 * nc);
     ilu_.sync = arena_.alloc<SweepSync>(2);
@@ -645,6 +676,7 @@ void Solver::ilu_factor() {
     h2d(ilu_.nbr, ilu_nbr_h_, s);
     h2d(ilu_.pos, ilu_pos_h_, s);
     h2d(ilu_.order, ilu_order_h_, s);
+    h2d(ilu_.sweep, ilu_sweep_h_, s);
     h2d(ilu_.lo_cells, lo_cells_h_, s);
     O2F_CUDA(cudaMemsetAsync(ilu_.flag, 0, 2 * nc * sizeof(uint32_t), s));
     O2F_CUDA(cudaMemsetAsync(ilu_.sync, 0, 2 * sizeof(SweepSync), s));
@@ -680,6 +712,16 @@ void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) 
   const int blocks = (chunks + warps_per_block - 1) / warps_per_block;
   k_ilu_sweep<true><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, r, z, gate);
   k_ilu_sweep<false><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, z, z, gate);
+}
+
+// Test hook: the next solves run their sweeps with `spin_limit` polls per
+// wait, and with `stall` the first row of the forward order never releases
+// its flag, so the rows that depend on it wait out their limit (no fault:
+// every wait is bounded).  spin_limit <= 0 and stall = 0 restore the
+// defaults.  Takes effect for the solves that start after the call.
+void Solver::debug_ilu_stall(int stall, long long spin_limit) {
+  ilu_.spin_limit = spin_limit > 0 ? spin_limit : kSweepSpinLimit;
+  ilu_.stall_row = stall && !ilu_sweep_h_.empty() ? ilu_sweep_h_[0] : -1;
 }
 
 // A sweep whose dependency wait ran out leaves an invalid result: report it

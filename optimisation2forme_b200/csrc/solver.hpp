@@ -185,7 +185,13 @@ class Solver {
   void ilu_factor();
   void ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate);
   void ilu_check_sweeps();
-  std::vector<int32_t> ilu_nbr_h_, ilu_pos_h_, ilu_order_h_, lo_off_h_, lo_cells_h_;
+
+ public:
+  void debug_ilu_stall(int stall, long long spin_limit);
+
+ private:
+  std::vector<int32_t> ilu_nbr_h_, ilu_pos_h_, ilu_order_h_, lo_off_h_, lo_cells_h_, ilu_sweep_h_;
+  int ilu_n_up_ = 0;  // levels of the backward sweep's dependencies
   IluDev ilu_{};
   bool ilu_alloc_ = false;
   int* ilu_status_ = nullptr;

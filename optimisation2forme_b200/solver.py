@@ -544,6 +544,12 @@ class Solver:
         check(lib().o2f_residual_norm_noalloc(self._h, C.byref(out)))
         return out.value
 
+    def debug_ilu_stall(self, stall: bool, spin_limit: int = 0) -> None:
+        """Test hook (o2f_debug_ilu_stall): the solves started afterwards run
+        their ILU sweeps with one row that never signals and `spin_limit`
+        polls per wait, so a bounded wait runs out; False / 0 restore."""
+        check(lib().o2f_debug_ilu_stall(self._h, int(bool(stall)), int(spin_limit)))
+
     def timing(self) -> dict:
         t = _lib.Timing()
         check(lib().o2f_get_timing(self._h, C.byref(t)))

@@ -1,6 +1,6 @@
 #!/bin/bash
 # Test infrastructure only: compiles the reference solver's OWN sources, read
-# in place from REF_DIR (default /root/reference), together with the shims in
+# in place from $REF_DIR (required: the reference checkout), together with the shims in
 # oracle/shims and the driver oracle/ref_harness.cpp, into oracle/_ref/.
 # Two flavours are built:
 #   o2f_ref_exact  -O2 -ffp-contract=off   parity oracle (no fused multiply-add)
@@ -9,7 +9,7 @@
 # optimizeShape (lines 560-741 and 1017-): Eigen is not installed.  The
 # extract is generated under oracle/_ref/ and never committed.
 set -euo pipefail
-REF_DIR=${REF_DIR:-/root/reference}
+REF_DIR=${REF_DIR:?set REF_DIR to the reference checkout}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 if [ ! -f "$REF_DIR/src/advection.cpp" ]; then

@@ -14,7 +14,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF_DIR = Path(os.environ.get("O2F_REFERENCE_DIR", "/root/reference"))
+# The reference checkout: $O2F_REFERENCE_DIR, else a directory named
+# "reference" beside this repository's checkout.
+REF_DIR = Path(os.environ.get("O2F_REFERENCE_DIR", str(HERE.parent.parent / "reference")))
 EXE_EXACT = HERE / "_ref" / "o2f_ref_exact"
 EXE_FAST = HERE / "_ref" / "o2f_ref_fast"
 

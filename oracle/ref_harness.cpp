@@ -23,6 +23,13 @@
 //   perturb <name> <eps>      applyShapePerturbationNACA12 geometry
 //   march <nsteps>            the SSP-RK3 time loop for nsteps steps
 //   bench <reps>              timings of computeResidual / applyJacobianTranspose
+//   eval <steps> <iters> <thermal>
+//                             one reduced shape-gradient evaluation, timed by
+//                             phase: <steps> SSP-RK3 steps (diffusive dt bound
+//                             with the thermal diffusivity when <thermal> is 1),
+//                             J and the adjoint right-hand side, <iters>
+//                             identity-preconditioned BiCGSTAB iterations on
+//                             applyJacobianTranspose, computeShapeGradient
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -186,10 +193,14 @@ void residual(Mesh& m, const SimulationParams& p) {
 // (src/simulation.cpp:68-171) without the SFML output step and without the
 // config reload.  Records per step: dt, t, and the L2 norm of R_rho of the
 // first stage (the residual of the state at the start of the step).
-void march(Mesh& mesh, const SimulationParams& p, int nsteps) {
+void march_core(Mesh& mesh, const SimulationParams& p, int nsteps, bool thermal, std::vector<double>& dts,
+                std::vector<double>& ts, std::vector<double>& rnorm) {
   double t = 0.0;
   int it = 0;
-  std::vector<double> dts, ts, rnorm;
+  // Thermal bound (no reference counterpart): the diffusive limit with the
+  // heat flux's effective diffusivity kappa*(gamma-1) when it exceeds mu.
+  const double mu_dt =
+      thermal ? std::max(p.viscosity, p.viscosity * p.cp / p.Pr * (p.gamma - 1.0)) : p.viscosity;
   while (t < p.final_time && it < nsteps) {
     double max_wave = 1e-8;
     double min_h = std::numeric_limits<double>::infinity();
@@ -208,7 +219,7 @@ void march(Mesh& mesh, const SimulationParams& p, int nsteps) {
       min_h = std::min(min_h, h);
     }
     double dt_adv = p.cfl_number * min_h / max_wave;
-    double dt_diff = 0.5 * (min_h * min_h) / p.viscosity;
+    double dt_diff = 0.5 * (min_h * min_h) / mu_dt;
     double dt = std::min(dt_adv, dt_diff);
     for (auto& c : mesh.cells) {
       c.rho_old = c.rho;
@@ -238,6 +249,11 @@ void march(Mesh& mesh, const SimulationParams& p, int nsteps) {
     ts.push_back(t);
     ++it;
   }
+}
+
+void march(Mesh& mesh, const SimulationParams& p, int nsteps) {
+  std::vector<double> dts, ts, rnorm;
+  march_core(mesh, p, nsteps, false, dts, ts, rnorm);
   dump_f64("march_dt", dts);
   dump_f64("march_t", ts);
   dump_f64("march_rnorm", rnorm);
@@ -246,6 +262,73 @@ void march(Mesh& mesh, const SimulationParams& p, int nsteps) {
 
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// y = J^T x through the reference's applyJacobianTranspose, vectors
+// interleaved 4*i+k as the reference's JacobianOpT packs them
+// (src/shape_optimization.cpp:616-629).
+struct JtOp {
+  Mesh& mesh;
+  const SimulationParams& p;
+  std::vector<double> xr, xru, xrv, xE, yr, yru, yrv, yE;
+  JtOp(Mesh& m, const SimulationParams& pp, std::size_t n)
+      : mesh(m), p(pp), xr(n), xru(n), xrv(n), xE(n), yr(n), yru(n), yrv(n), yE(n) {}
+  void operator()(const std::vector<double>& x, std::vector<double>& y) {
+    const std::size_t n = xr.size();
+#pragma omp parallel for
+    for (std::size_t i = 0; i < n; ++i) {
+      xr[i] = x[4 * i];
+      xru[i] = x[4 * i + 1];
+      xrv[i] = x[4 * i + 2];
+      xE[i] = x[4 * i + 3];
+    }
+    applyJacobianTranspose(mesh, p, xr, xru, xrv, xE, yr, yru, yrv, yE, 1e-6);
+#pragma omp parallel for
+    for (std::size_t i = 0; i < n; ++i) {
+      y[4 * i] = yr[i];
+      y[4 * i + 1] = yru[i];
+      y[4 * i + 2] = yrv[i];
+      y[4 * i + 3] = yE[i];
+    }
+  }
+};
+
+double dot(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0.0;
+#pragma omp parallel for reduction(+ : s)
+  for (std::size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+  return s;
+}
+
+// `iters` iterations of identity-preconditioned BiCGSTAB (van der Vorst,
+// 1992) on J^T lambda = b from lambda = 0, the algorithm the reference calls
+// from Eigen (src/shape_optimization.cpp:699-716); returns ||r|| / ||b|| of
+// the recurrence residual.
+double bicgstab_iters(JtOp& A, const std::vector<double>& b, int iters, std::vector<double>& x) {
+  const std::size_t n = b.size();
+  std::vector<double> r = b, r0 = b, p(n, 0.0), v(n, 0.0), s(n), t(n);
+  x.assign(n, 0.0);
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  const double bn = std::sqrt(dot(b, b));
+  for (int it = 0; it < iters; ++it) {
+    const double rho_new = dot(r0, r);
+    const double beta = (rho_new / rho) * (alpha / omega);
+#pragma omp parallel for
+    for (std::size_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+    A(p, v);
+    alpha = rho_new / dot(r0, v);
+#pragma omp parallel for
+    for (std::size_t i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+    A(s, t);
+    omega = dot(t, s) / dot(t, t);
+#pragma omp parallel for
+    for (std::size_t i = 0; i < n; ++i) {
+      x[i] += alpha * p[i] + omega * s[i];
+      r[i] = s[i] - omega * t[i];
+    }
+    rho = rho_new;
+  }
+  return std::sqrt(dot(r, r)) / (bn > 0 ? bn : 1.0);
 }
 
 }  // namespace
@@ -322,6 +405,40 @@ int main(int argc, char** argv) {
       dump_residual_outputs(mesh, params, beta);
     } else if (mode == "march") {
       march(mesh, params, std::atoi(argv[4]));
+    } else if (mode == "eval") {
+      const int nsteps = std::max(0, std::atoi(argv[4]));
+      const int iters = std::max(0, std::atoi(argv[5]));
+      const bool thermal = argc > 6 && std::atoi(argv[6]) != 0;
+      residual(mesh, params);  // sizes the static scratch buffers (not timed)
+      std::vector<double> dts, ts, rnorm;
+      const double t0 = now_s();
+      march_core(mesh, params, nsteps, thermal, dts, ts, rnorm);
+      const double t1 = now_s();
+      residual(mesh, params);
+      double CL = 0, CD = 0;
+      computeLiftDragCoefficients(mesh, params, CL, CD);
+      const double J = computeDirectObjectiveTerm(mesh, params, beta);
+      std::vector<double> br, bru, brv, bE;
+      assembleAdjointRHS(mesh, params, br, bru, brv, bE, beta);
+      std::vector<double> b(4 * nc), lambda;
+      for (std::size_t i = 0; i < nc; ++i) {
+        b[4 * i] = br[i];
+        b[4 * i + 1] = bru[i];
+        b[4 * i + 2] = brv[i];
+        b[4 * i + 3] = bE[i];
+      }
+      const double t2 = now_s();
+      JtOp op(mesh, params, nc);
+      const double relres = bicgstab_iters(op, b, iters, lambda);
+      const double t3 = now_s();
+      std::vector<double> g;
+      computeShapeGradient(mesh, params, lambda, names_all, values_all, names, g, beta, 1e-6);
+      const double t4 = now_s();
+      std::printf("{\"cells\": %zu, \"threads\": %d, \"steps\": %d, \"iters\": %d, \"steps_s\": %.9g, "
+                  "\"objective_s\": %.9g, \"bicgstab_s\": %.9g, \"gradient_s\": %.9g, \"total_s\": %.9g, "
+                  "\"J\": %.17g, \"relres\": %.9g, \"n_params\": %zu}\n",
+                  nc, omp_get_max_threads(), nsteps, iters, t1 - t0, t2 - t1, t3 - t2, t4 - t3, t4 - t0, J, relres,
+                  g.size());
     } else if (mode == "bench") {
       // Per-call wall times of the reference's computeResidual and
       // applyJacobianTranspose, `reps` samples each (the first residual call

@@ -85,3 +85,27 @@ def test_call_order_is_checked():
         assert e.value.status == "O2F_ERR_STATE"
         with pytest.raises(ValueError):
             s.set_state(np.zeros(5))
+
+
+def test_ilu_sweep_wait_that_runs_out_returns_a_status():
+    """The ILU(0) sweeps wait, bounded, on the ready flags of the rows they
+    depend on.  A row made never to signal (test hook) lets its dependants'
+    waits run out: the solve returns O2F_ERR_CUDA instead of hanging, and
+    after the hook is cleared the same context solves to the same lambda as
+    before."""
+    from optimisation2forme_b200 import O2FError
+    s, p = _solver()
+    with s:
+        s.initialize_freestream()
+        s.time_loop(50)
+        s.compute_residual()
+        ref = s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=2000, restart=500)
+        s.debug_ilu_stall(True, spin_limit=1 << 12)
+        with pytest.raises(O2FError) as e:
+            s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=20, restart=10)
+        assert e.value.status == "O2F_ERR_CUDA"
+        assert "dependency wait" in str(e.value)
+        s.debug_ilu_stall(False)
+        again = s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=2000, restart=500)
+        assert again["iters"] == ref["iters"]
+        np.testing.assert_array_equal(again["lambda"], ref["lambda"])

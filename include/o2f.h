@@ -353,13 +353,16 @@ int o2f_profile_kernels(o2f_ctx* ctx, int reps, double* ms_out);
 
 /* Batched time loop (no reference counterpart: the reference solves one
  * candidate per process, run_opti.sh).  A batch references n existing
- * FP64 contexts (each with its own mesh, flow parameters and state; all on
- * one device, the batch runs on the first context's stream); the contexts
- * must outlive the batch and must not be used while a batch call runs.
+ * contexts of one precision, all O2F_PREC_F64 or all O2F_PREC_F32 (each with
+ * its own mesh, flow parameters and state; all on one device, the batch runs
+ * on the first context's stream); the contexts must outlive the batch, must
+ * not be used while a batch call runs and must keep their precision.
  * o2f_batch_rk3_run advances every candidate by SSP-RK3 exactly as
- * o2f_rk3_run would (bit-identical FP64 states, each candidate with its own
- * dt and stop condition) with one grouped launch per phase for the whole
- * batch, captured in a CUDA graph.  Per candidate: steps_done, t_out,
+ * o2f_rk3_run would (bit-identical states, each candidate with its own
+ * dt and stop condition; FP32 contexts run the mixed-precision residual and
+ * leave the FP64 linearisation of their last stage, as o2f_rk3_run does)
+ * with one grouped launch per phase for the whole batch, captured in a CUDA
+ * graph.  Per candidate: steps_done, t_out,
  * status_out (O2F_OK or O2F_ERR_NONFINITE); any may be NULL.  After the run
  * each context holds the interface states of its last stage, so
  * o2f_forces / o2f_adjoint_solve / o2f_shape_gradient apply per context. */
@@ -376,6 +379,8 @@ int o2f_batch_destroy(o2f_batch* batch);
 int o2f_batch_tune(o2f_batch* batch, int reps, int* config_out);
 int o2f_batch_rk3_run(o2f_batch* batch, int64_t max_steps, double drop_tol, int64_t* steps_done, double* t_out,
                       int* status_out);
+/* Kernels launched by the batch so far (grouped phases and step kernels). */
+int o2f_batch_launches(o2f_batch* batch, int64_t* launches);
 /* ||R_rho||_2 history of candidate `index` from the last o2f_batch_rk3_run. */
 int o2f_batch_history(o2f_batch* batch, int index, double* history_host, int64_t count);
 

@@ -164,6 +164,7 @@ SIGNATURES = {
     "o2f_batch_tune": ([_vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "o2f_batch_rk3_run": ([_vp, C.c_int64, C.c_double, C.POINTER(C.c_int64), _dp, C.POINTER(C.c_int)], C.c_int),
     "o2f_batch_history": ([_vp, C.c_int, _dp, C.c_int64], C.c_int),
+    "o2f_batch_launches": ([_vp, C.POINTER(C.c_int64)], C.c_int),
 }
 
 KERNEL_CLASSES = ["vertex_state", "cell_gradient", "vertex_visc", "edge_flux", "cell_residual", "jt_apply",

@@ -431,6 +431,13 @@ int o2f_batch_rk3_run(o2f_batch* batch, int64_t max_steps, double drop_tol, int6
   return guarded([&] { B(batch).rk3_run(max_steps, drop_tol, steps_done, t_out, status_out); });
 }
 
+int o2f_batch_launches(o2f_batch* batch, int64_t* launches) {
+  return guarded([&] {
+    need(launches, "launches");
+    *launches = B(batch).launches();
+  });
+}
+
 int o2f_batch_history(o2f_batch* batch, int index, double* history_host, int64_t count) {
   return guarded([&] {
     need(history_host, "history");

@@ -50,9 +50,13 @@ Batch::Batch(std::vector<Solver*> solvers) : s_(std::move(solvers)) {
   if (s_.empty()) throw Error(O2F_ERR_ARG, "empty batch");
   if (s_.size() > 4096) throw Error(O2F_ERR_ARG, "at most 4096 candidates per batch");
   stream_ = s_[0]->stream_;
-  for (Solver* s : s_) {
+  for (Solver* s : s_)
     if (!s) throw Error(O2F_ERR_ARG, "null context in the batch");
-    if (s->params_.precision != O2F_PREC_F64) throw Error(O2F_ERR_ARG, "batched contexts must use O2F_PREC_F64");
+  f32_ = s_[0]->params_.precision == O2F_PREC_F32;
+  for (Solver* s : s_) {
+    if (s->params_.precision != s_[0]->params_.precision)
+      throw Error(O2F_ERR_ARG, "batched contexts must all use the same precision");
+    if (f32_) s->ensure_f32();  // the FP32 buffers the grouped kernels write
     total_cells_ += s->topo_.nc;
   }
   const int n = (int)s_.size();
@@ -68,11 +72,17 @@ Batch::Batch(std::vector<Solver*> solvers) : s_(std::move(solvers)) {
     it.st = s.step_;
     it.norm_part = arena_.alloc<double>((s.topo_.nc + 127) / 128);  // enough for any block >= 128
     it.hist = nullptr;
+    if (f32_) {
+      it.g32 = s.geom32_;
+      it.w32 = s.work32_;
+      it.U32 = s.U32_;
+      it.Ukeep = s.Ukeep_;
+    }
   }
   items_dev_ = arena_.alloc<BatchItem>(n);
   for (int p = 0; p < kBatchPhases; ++p) off_dev_[p] = arena_.alloc<int>(n + 1);
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  auto hit = g_tuned.find(bucket_of(total_cells_));
+  auto hit = g_tuned.find(2 * bucket_of(total_cells_) + (f32_ ? 1 : 0));
   for (int p = 0; p < kBatchPhases; ++p) cfg_[p] = hit != g_tuned.end() ? hit->second[p] : BatchCfg{256, 1};
   layout();
 }
@@ -96,7 +106,8 @@ void Batch::layout() {
 
 void Batch::upload_items() {
   for (size_t i = 0; i < s_.size(); ++i) {
-    if (s_[i]->params_.precision != O2F_PREC_F64) throw Error(O2F_ERR_ARG, "batched contexts must use O2F_PREC_F64");
+    if (s_[i]->params_.precision != (f32_ ? O2F_PREC_F32 : O2F_PREC_F64))
+      throw Error(O2F_ERR_ARG, "a batched context changed its precision");
     items_h_[i].ph = s_[i]->phys_;
   }
   O2F_CUDA(cudaMemcpyAsync(items_dev_, items_h_.data(), items_h_.size() * sizeof(BatchItem), cudaMemcpyHostToDevice,
@@ -104,10 +115,15 @@ void Batch::upload_items() {
   O2F_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Batch::launch_phase(int p, bool rk, const RkStage& stage) {
+void Batch::launch_phase(int p, bool rk, const RkStage& stage, bool keep) {
   const int n = (int)s_.size();
   const int B = cfg_[p].block, T = cfg_[p].tile, G = blocks_[p];
   if (G == 0) return;
+  if (f32_ && p != kPhWave) {
+    batch_launch_mixed(p, rk, stage, keep, items_dev_, n, off_dev_[p], G, B, T, stream_);
+    ++launches_;
+    return;
+  }
   switch (p) {
     case kPhVertexState:
       kb_phase<kPhVertexState, false><<<G, B, 0, stream_>>>(items_dev_, n, off_dev_[p], T, stage);
@@ -136,8 +152,9 @@ void Batch::launch_phase(int p, bool rk, const RkStage& stage) {
   ++launches_;
 }
 
-void Batch::launch_residual(const RkStage* rk) {
-  for (int p = kPhVertexState; p <= kPhCellResidual; ++p) launch_phase(p, rk != nullptr, rk ? *rk : RkStage{});
+void Batch::launch_residual(const RkStage* rk, bool keep) {
+  for (int p = kPhVertexState; p <= kPhCellResidual; ++p)
+    launch_phase(p, rk != nullptr, rk ? *rk : RkStage{}, keep);
 }
 
 // StepState of every candidate for a new loop, as Solver::rk3_run sets it.
@@ -162,7 +179,15 @@ void Batch::tune(int reps, int* cfg_out) {
   // Valid inputs for every phase: one residual of each candidate's state,
   // with running step states (the grouped kernels skip stopped candidates).
   init_steps(1, 0.0);
-  for (Solver* s : s_) s->launch_residual(s->geom_, s->work_, s->U_, nullptr, false, nullptr);
+  for (Solver* s : s_) {
+    if (f32_) {
+      s->ensure_f32();
+      s->f32_state_sync();
+      s->launch_residual_f32(nullptr, nullptr);
+    } else {
+      s->launch_residual(s->geom_, s->work_, s->U_, nullptr, false, nullptr);
+    }
+  }
   static const int kBlocks[] = {128, 256, 512};
   static const int kTiles[] = {1, 2, 4};
   cudaEvent_t e0, e1;
@@ -194,7 +219,7 @@ void Batch::tune(int reps, int* cfg_out) {
   layout();
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tuned[bucket_of(total_cells_)] = best;
+    g_tuned[2 * bucket_of(total_cells_) + (f32_ ? 1 : 0)] = best;
   }
   for (Solver* s : s_) {
     s->have_residual_ = true;
@@ -217,6 +242,11 @@ void Batch::rk3_run(int64_t max_steps, double drop_tol, int64_t* steps_done, dou
   }
   upload_items();  // flow parameters may have changed since the batch was made
   init_steps(max_steps, drop_tol);
+  if (f32_)  // FP32 geometry (refreshed if the parameters changed) and state shadow
+    for (Solver* s : s_) {
+      s->ensure_f32();
+      s->f32_state_sync();
+    }
   const RkStage s1{0.0, 1.0, nullptr, 1, items_h_[0].norm_part};  // norm_part: flag only
   const RkStage s2{3.0 / 4.0, 1.0 / 4.0, nullptr, 0, nullptr};
   const RkStage s3{1.0 / 3.0, 2.0 / 3.0, nullptr, 0, nullptr};
@@ -232,7 +262,7 @@ void Batch::rk3_run(int64_t max_steps, double drop_tol, int64_t* steps_done, dou
     launch_residual(&s1);
     kb_step_norm<<<n, 1024, 0, stream_>>>(items_dev_, n);
     launch_residual(&s2);
-    launch_residual(&s3);
+    launch_residual(&s3, true);
     kb_step_end<<<sgrid, 128, 0, stream_>>>(items_dev_, n);
     launches_ += 4;
   }
@@ -265,9 +295,13 @@ void Batch::rk3_run(int64_t max_steps, double drop_tol, int64_t* steps_done, dou
     if (steps_done) steps_done[i] = host[i].step;
     if (t_out) t_out[i] = host[i].t;
     if (status) status[i] = host[i].stop == 2 ? O2F_ERR_NONFINITE : O2F_OK;
+    // FP32 contexts: the linearisation's FP64 interface states about the
+    // last stage's input state, as Solver::rk3_run leaves them.
+    if (f32_ && host[i].step > 0) s.launch_residual(s.geom_, s.work_, s.Ukeep_, nullptr, false, nullptr);
     s.have_residual_ = host[i].step > 0;
     s.invalidate_linearisation();
   }
+  if (f32_) O2F_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Batch::history(int i, double* out, int64_t count) {

@@ -22,12 +22,26 @@ struct BatchItem {
   double* norm_part;  // per-block partial sums of R_rho^2 (the batch's own array)
   double* hist;       // residual history (the batch's own array)
   int nparts;         // blocks of this candidate in the stage-1 cell phase
+  // FP32 contexts (mixed precision): FP32 geometry, residual buffers and
+  // state shadow, and the FP64 input state of the last RK3 stage
+  Geom<float> g32;
+  Work<float> w32;
+  Vec4<float>* U32;
+  Vec4<double>* Ukeep;
 };
 
 // Phases of one RK3 stage plus the wave-speed reduction, each one grouped
 // launch over the batch.
 enum BatchPhase { kPhVertexState = 0, kPhCellGradient, kPhVertexVisc, kPhEdgeFlux, kPhCellResidual, kPhWave };
 constexpr int kBatchPhases = 6;
+
+// One grouped launch of a residual phase (kPhVertexState .. kPhCellResidual)
+// over a batch of FP32 contexts: the FP32 per-entity functions of their own
+// Solver::rk3_run, in a translation unit compiled like theirs (solver_f32.cu).
+// keep: the cell phase stores each candidate's FP64 input state in Ukeep.
+struct RkStage;
+void batch_launch_mixed(int phase, bool rk, const RkStage& stage, bool keep, const BatchItem* items, int n,
+                        const int* off, int grid, int block, int tile, cudaStream_t stream);
 
 struct BatchCfg {
   int block;  // threads per block: 128, 256 or 512
@@ -48,8 +62,8 @@ class Batch {
   void layout();
   void upload_items();
   void init_steps(int64_t max_steps, double drop_tol);
-  void launch_phase(int phase, bool rk, const RkStage& stage);
-  void launch_residual(const RkStage* rk);
+  void launch_phase(int phase, bool rk, const RkStage& stage, bool keep = false);
+  void launch_residual(const RkStage* rk, bool keep = false);
 
   std::vector<Solver*> s_;
   cudaStream_t stream_ = nullptr;
@@ -60,6 +74,7 @@ class Batch {
   int* off_dev_[kBatchPhases]{};
   int blocks_[kBatchPhases]{};
   int64_t total_cells_ = 0;
+  bool f32_ = false;  // the contexts run the mixed-precision residual
   int64_t hist_cap_ = 0;
   int64_t launches_ = 0;
 };

@@ -887,9 +887,18 @@ void Solver::profile_kernels(int reps, double* ms_out) {
   if (!tmp_) tmp_ = arena_.alloc<Vec4<double>>(topo_.nc);
   if (!s_) s_ = arena_.alloc<Vec4<double>>(topo_.nc);
   O2F_CUDA(cudaMemsetAsync(s_, 0, topo_.nc * sizeof(Vec4<double>), s));
+  if (f32()) {  // the residual kernels of this context's precision
+    ensure_f32();
+    f32_state_sync();
+    launch_residual_f32(nullptr, nullptr);
+  }
   for (int k = 0; k < O2F_K_COUNT; ++k) {
     O2F_CUDA(cudaEventRecord(ev0_, s));
     for (int r = 0; r < reps; ++r) {
+      if (f32() && k <= O2F_K_CELL_RESIDUAL) {
+        profile_kernel_f32(k);
+        continue;
+      }
       switch (k) {
         case O2F_K_VERTEX_STATE:
           k_vertex_state<double><<<grid(t.nv), kBlock, 0, s>>>(t.nv, t.voff, t.vcid, g.vw, t.vbc, U_, phys_, w.vq,

@@ -137,6 +137,7 @@ class Solver {
   void f32_state_sync();
   void f32_publish_interfaces();
   void launch_residual_f32(const int* gate, const void* rk, Vec4<double>* keep = nullptr);
+  void profile_kernel_f32(int k);  // one launch of residual kernel class k (O2F_K_*) in FP32
   void f32_blocks();
   void to_internal(const double* ref, Vec4<double>* dev);
   void to_reference(const Vec4<double>* dev, double* ref);

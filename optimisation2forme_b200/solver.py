@@ -557,11 +557,12 @@ class Solver:
 
 
 class Batch:
-    """Several FP64 Solver contexts advanced together by the batched time loop
-    (o2f_batch_*): one grouped launch per phase of each SSP-RK3 step for all
-    candidates, each candidate with its own mesh, flow parameters, dt and stop
-    condition, and the same FP64 states as Solver.time_loop.  The contexts must
-    outlive the batch."""
+    """Several Solver contexts of one precision (all FP64 or all FP32)
+    advanced together by the batched time loop (o2f_batch_*): one grouped
+    launch per phase of each SSP-RK3 step for all candidates, each candidate
+    with its own mesh, flow parameters, dt and stop condition, and the same
+    states as its own Solver.time_loop.  The contexts must outlive the
+    batch."""
 
     PHASES = ("vertex_state", "cell_gradient", "vertex_visc", "edge_flux", "cell_residual", "wave_speed")
 
@@ -585,6 +586,11 @@ class Batch:
         st = (C.c_int * n)()
         check(lib().o2f_batch_rk3_run(self._h, int(max_steps), float(residual_drop), steps, _ptr(t), st))
         return [{"steps": steps[i], "t": float(t[i]), "status": _lib.STATUS.get(st[i], "OK")} for i in range(n)]
+
+    def launches(self) -> int:
+        n = C.c_int64()
+        check(lib().o2f_batch_launches(self._h, C.byref(n)))
+        return n.value
 
     def history(self, index: int, count: int) -> np.ndarray:
         out = np.empty(max(int(count), 1))

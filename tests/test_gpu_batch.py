@@ -146,3 +146,45 @@ def test_poisoned_candidate_fails_alone():
     finally:
         for s in ctxs:
             s.close()
+
+
+def test_batched_mixed_precision_is_bit_identical_to_single_fp32_contexts():
+    """A batch of FP32 (mixed-precision) contexts: the grouped FP32 residual
+    phases advance every candidate exactly as its own context's FP32 time
+    loop, and leave the same FP64 linearisation (forces, adjoint RHS)."""
+    from optimisation2forme_b200 import Batch, Solver
+    ref = []
+    for mk, pk in CANDIDATES:
+        with Solver(_params(precision="fp32", **pk), desc=desc_of(small_mesh(**mk))) as s:
+            s.initialize_freestream()
+            r = s.time_loop(30)
+            ref.append((s.get_state(), r, s.lift_drag(0.1), s.assemble_adjoint_rhs(0.1)))
+    ctxs = [Solver(_params(precision="fp32", **pk), desc=desc_of(small_mesh(**mk))) for mk, pk in CANDIDATES]
+    try:
+        for s in ctxs:
+            s.initialize_freestream()
+        with Batch(ctxs) as b:
+            b.tune(reps=2)
+            for s in ctxs:
+                s.initialize_freestream()
+            res = b.time_loop(30)
+            assert b.launches() > 0
+            for i, s in enumerate(ctxs):
+                U, r, forces, rhs = ref[i]
+                assert res[i]["status"] == "OK" and res[i]["steps"] == r["steps"] == 30
+                assert res[i]["t"] == r["t"]
+                assert bits_equal(s.get_state(), U)
+                assert s.lift_drag(0.1) == forces
+                assert bits_equal(s.assemble_adjoint_rhs(0.1), rhs)
+    finally:
+        for s in ctxs:
+            s.close()
+
+
+def test_batch_rejects_mixed_precisions():
+    from optimisation2forme_b200 import Batch, O2FError, Solver
+    (mk0, pk0), (mk1, pk1) = CANDIDATES[0], CANDIDATES[1]
+    with Solver(_params(**pk0), desc=desc_of(small_mesh(**mk0))) as a, \
+            Solver(_params(precision="fp32", **pk1), desc=desc_of(small_mesh(**mk1))) as b:
+        with pytest.raises(O2FError):
+            Batch([a, b])

@@ -411,6 +411,31 @@ int o2f_mlp_gradients(o2f_mlp* net, const float* inputs, const float* targets, i
 int o2f_mlp_get_params(o2f_mlp* net, float* params, float* freq);
 int o2f_mlp_set_params(o2f_mlp* net, const float* params);
 
+/* Array forms of the reference's per-edge and per-state functions, which the
+ * reference calls one edge or one state at a time inside its loops; n of
+ * them per call, evaluated on the GPU by the residual's own device functions
+ * (same bits as the reference).  Host arrays in, host arrays out; no context.
+ *
+ * o2f_hllc_flux: compute_hllc_flux (src/advection.cpp:335-412;
+ * include/advection.hpp:16).  LR_host[8*i..8*i+7] = rho_L, rho_u_L, rho_v_L,
+ * E_L, rho_R, rho_u_R, rho_v_R, E_R of edge i, normal_host[2*i..] its
+ * Edge::edgeNormal (nx, ny); flux_host[4*i..] receives the four fluxes. */
+int o2f_hllc_flux(int64_t n, const double* LR_host, const double* normal_host, double gamma, double* flux_host);
+/* apply_boundary_conditions for "inflow_outflow_x" (src/boundary.cpp:7-45,
+ * 84-94; include/boundary.hpp:13): U_host[4*i..] (rho, rho_u, rho_v, E) is
+ * replaced by the boundary state of code codes[i] (O2F_BC_*; other codes
+ * leave it).  The freestream comes from params (inflow_velocity, rho_ref,
+ * p_ref, gamma; aoa_deg 0 is the reference). */
+int o2f_bc_states(const o2f_params* params, int64_t n, const uint8_t* codes, double* U_host);
+/* apply_InterfaceStates_boundary_conditions (src/boundary.cpp:48-80;
+ * include/boundary.hpp:17-20): the ghost right state R_host[4*i..] of a
+ * boundary edge from its left state L_host[4*i..]. */
+int o2f_bc_ghosts(const o2f_params* params, int64_t n, const uint8_t* codes, const double* L_host, double* R_host);
+/* apply_diffusion_bc (src/boundary.cpp:101-127; include/boundary.hpp:15):
+ * tq_host[5*i..] = tau_xx, tau_yy, tau_xy, q_x, q_y, zeroed for far-field
+ * and wall codes. */
+int o2f_bc_diffusion(int64_t n, const uint8_t* codes, double* tq_host);
+
 /* Test hook of the failure path (no counterpart in the reference).  The
  * block-ILU(0) sweeps wait, bounded, on the ready flags of the rows they
  * depend on; a wait that runs out makes the solve return O2F_ERR_CUDA and

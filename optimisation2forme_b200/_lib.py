@@ -140,6 +140,10 @@ SIGNATURES = {
     "o2f_profile_kernels": ([_vp, C.c_int, _dp], C.c_int),
     "o2f_residual_norm_noalloc": ([_vp, _dp], C.c_int),
     "o2f_debug_ilu_stall": ([_vp, C.c_int, C.c_int64], C.c_int),
+    "o2f_hllc_flux": ([C.c_int64, _dp, _dp, C.c_double, _dp], C.c_int),
+    "o2f_bc_states": ([C.POINTER(Params), C.c_int64, C.POINTER(C.c_uint8), _dp], C.c_int),
+    "o2f_bc_ghosts": ([C.POINTER(Params), C.c_int64, C.POINTER(C.c_uint8), _dp, _dp], C.c_int),
+    "o2f_bc_diffusion": ([C.c_int64, C.POINTER(C.c_uint8), _dp], C.c_int),
     "o2f_host_mesh_set_coords": ([_vp, _dp], C.c_int),
     "o2f_checkpoint_write": ([C.c_char_p, C.c_int64, _dp, C.c_double, C.c_int64], C.c_int),
     "o2f_checkpoint_read": ([C.c_char_p, C.c_int64, _dp, _dp, C.POINTER(C.c_int64)], C.c_int),

@@ -516,6 +516,53 @@ int o2f_mlp_set_params(o2f_mlp* net, const float* params) {
   });
 }
 
+int o2f_hllc_flux(int64_t n, const double* LR_host, const double* normal_host, double gamma, double* flux_host) {
+  return guarded([&] {
+    if (n > 0) {
+      need(LR_host, "LR_host");
+      need(normal_host, "normal_host");
+      need(flux_host, "flux_host");
+    }
+    o2f::hllc_points(n, LR_host, normal_host, gamma, flux_host);
+  });
+}
+
+int o2f_bc_states(const o2f_params* params, int64_t n, const uint8_t* codes, double* U_host) {
+  return guarded([&] {
+    need(params, "params");
+    if (n > 0) {
+      need(codes, "codes");
+      need(U_host, "U_host");
+    }
+    o2f::bc_points(0, *params, n, codes, U_host, nullptr);
+  });
+}
+
+int o2f_bc_ghosts(const o2f_params* params, int64_t n, const uint8_t* codes, const double* L_host, double* R_host) {
+  return guarded([&] {
+    need(params, "params");
+    if (n > 0) {
+      need(codes, "codes");
+      need(L_host, "L_host");
+      need(R_host, "R_host");
+    }
+    std::vector<double> L(L_host, L_host + 4 * std::max<int64_t>(n, 0));
+    o2f::bc_points(1, *params, n, codes, L.data(), R_host);
+  });
+}
+
+int o2f_bc_diffusion(int64_t n, const uint8_t* codes, double* tq_host) {
+  return guarded([&] {
+    if (n > 0) {
+      need(codes, "codes");
+      need(tq_host, "tq_host");
+    }
+    o2f_params p;
+    o2f_params_default(&p);
+    o2f::bc_points(2, p, n, codes, tq_host, nullptr);
+  });
+}
+
 int o2f_debug_ilu_stall(o2f_ctx* ctx, int stall, int64_t spin_limit) {
   return guarded([&] { S(ctx).debug_ilu_stall(stall, (long long)spin_limit); });
 }

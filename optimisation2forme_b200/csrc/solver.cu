@@ -41,7 +41,7 @@ void h2d(X* dst, const std::vector<X>& src, cudaStream_t s) {
 }
 
 void validate_params(const o2f_params& p) {
-  if (!(p.gamma > 1.0) || !(p.viscosity > 0.0) || !(p.Pr > 0.0) || !(p.cp > 0.0) || !(p.rho_ref > 0.0) ||
+  if (!(p.gamma > 1.0) || !(p.viscosity >= 0.0) || !(p.Pr > 0.0) || !(p.cp > 0.0) || !(p.rho_ref > 0.0) ||
       !(p.p_ref > 0.0) || !(p.cfl_number > 0.0) || !(p.inflow_velocity >= 0.0) || !(p.limiter_k > 0.0))
     throw Error(O2F_ERR_ARG, "invalid physical parameters");
   if (p.limiter != O2F_LIMITER_VENKAT && p.limiter != O2F_LIMITER_BARTH_JESPERSEN)
@@ -115,8 +115,9 @@ Solver::~Solver() {
 
 void Solver::sync() { O2F_CUDA(cudaStreamSynchronize(stream_)); }
 
-void Solver::compute_phys() {
-  const o2f_params& p = params_;
+void Solver::compute_phys() { phys_ = phys_of(params_); }
+
+Phys phys_of(const o2f_params& p) {
   Phys ph{};
   ph.gamma = p.gamma;
   ph.mu = p.viscosity;
@@ -147,7 +148,7 @@ void Solver::compute_phys() {
   ph.q_inf = 0.5 * (rho0 * U_inf * U_inf);
   ph.limiter_k = p.limiter_k;
   ph.limiter = p.limiter;
-  phys_ = ph;
+  return ph;
 }
 
 void Solver::set_params(const o2f_params& p) {

@@ -44,6 +44,15 @@ struct TopologyLimit : Error {
 constexpr int64_t kGpuTopologyCells = 100000;
 
 void cuda_check(cudaError_t e, const char* what);
+
+// Physical constants of the kernels from the parameters: freestream (rotated
+// by the angle of attack), diffusivities, limiter.
+Phys phys_of(const o2f_params& p);
+
+// Array forms of the reference's per-edge / per-state functions (pointwise.cu).
+void hllc_points(int64_t n, const double* LR_host, const double* normal_host, double gamma, double* flux_host);
+void bc_points(int kind, const o2f_params& p, int64_t n, const uint8_t* codes_host, double* inout_host,
+               double* out_host);
 #define O2F_CUDA(x) ::o2f::cuda_check((x), #x)
 
 // Owning device allocation list.

@@ -37,4 +37,18 @@ build() {
 }
 build exact -O2 -ffp-contract=off
 build fast -O3 -march=x86-64-v3
+# The link check of the drop-in adapter: the reference's exact objects (its
+# own harness left out), the adapter under another namespace, libo2f.so.
+PKG=$(cd "$HERE/../optimisation2forme_b200" && pwd)
+if [ -f "$PKG/libo2f.so" ]; then
+  g++ -std=c++17 -fopenmp -w -O2 -ffp-contract=off -DO2F_ADAPTER_NS=o2f_adapter $INC -I"$HERE/../include" \
+    -c "$PKG/adapters/navier_stokes_o2f.cpp" -o "$OUT/obj_exact/adapter_o2f.o"
+  g++ -std=c++17 -fopenmp -w -O2 -ffp-contract=off $INC -c "$HERE/adapter_check.cpp" -o "$OUT/obj_exact/adapter_check.o"
+  REFOBJS=""
+  for s in advection diffusion boundary compute mesh utils params init shape_optimization_noeigen; do
+    REFOBJS="$REFOBJS $OUT/obj_exact/$s.o"
+  done
+  g++ -fopenmp $REFOBJS "$OUT/obj_exact/adapter_o2f.o" "$OUT/obj_exact/adapter_check.o" -L"$PKG" -lo2f \
+    -Wl,-rpath,'$ORIGIN/../../optimisation2forme_b200' -o "$OUT/o2f_adapter_check"
+fi
 echo "built $OUT/o2f_ref_exact $OUT/o2f_ref_fast"

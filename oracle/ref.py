@@ -21,8 +21,11 @@ EXE_EXACT = HERE / "_ref" / "o2f_ref_exact"
 EXE_FAST = HERE / "_ref" / "o2f_ref_fast"
 
 
+EXE_ADAPTER = HERE / "_ref" / "o2f_adapter_check"
+
+
 def available() -> bool:
-    return EXE_EXACT.exists()
+    return EXE_EXACT.exists() and EXE_ADAPTER.exists()
 
 
 def build() -> bool:

@@ -1,0 +1,39 @@
+"""The drop-in C++ adapter, linked and run against the reference's own
+compiled code: oracle/_ref/o2f_adapter_check holds the reference's
+translation units and the adapter (under its own namespace) in one binary,
+builds the reference Mesh of the shipped fixture with its state, and compares
+what each side leaves in the Mesh, bit for bit: computeAdvectionTerm +
+computeDiffusionTerm, computeResidual, computeLiftDragCoefficients,
+compute_hllc_flux on every edge and the three boundary functions.  The
+binary is built with the reference build (oracle/build_ref.sh) where the
+reference sources are present; the test skips without it."""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+
+import pytest
+
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.skipif(not ref.EXE_ADAPTER.exists(), reason="oracle/_ref/o2f_adapter_check not built")
+def test_adapter_matches_the_reference_bit_for_bit(golden_dir, tmp_path):
+    cfg = ref.write_config(tmp_path / "cfg.txt", mesh=str(golden_dir / "naca_2D_shape_0.msh"),
+                           state=str(golden_dir / "naca_2D_flow_1"), viscosity=1.8e-5, inflow_velocity=0.3,
+                           cfl=0.5, final_time=0.005)
+    r = subprocess.run([str(ref.EXE_ADAPTER), str(cfg)], capture_output=True, text=True, cwd=tmp_path,
+                       env={**os.environ, "OMP_NUM_THREADS": "1"}, timeout=600)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert lines, r.stdout + r.stderr
+    out = json.loads(lines[-1])
+    print("\nadapter vs reference:", out)
+    assert out["cells"] == 25274
+    for k in ("advection_cells", "advection_edges", "residual_cells", "residual_edges", "compute_residual", "hllc",
+              "bc"):
+        assert out[k] == 0, k
+    assert out["force_rel_err"] <= 1e-12
+    assert r.returncode == 0

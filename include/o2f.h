@@ -129,6 +129,11 @@ typedef struct o2f_params {
                              adjoint (default REFERENCE)                        */
   double adjoint_fd_step; /* NEW: relative step of the FULL Jacobian's central
                              differences (default 1e-9)                         */
+  int adjoint_precision;  /* NEW: O2F_PREC_F32 streams the Jacobian blocks of the
+                             BiCGSTAB products in FP32, every restart taking the
+                             true residual with the FP64 operator (iterative
+                             refinement: same solution and tolerance); F64
+                             default.  FP32 contexts always do this.             */
 } o2f_params;
 
 void o2f_params_default(o2f_params* p);

@@ -60,6 +60,7 @@ class Params(C.Structure):
         ("verbosity", C.c_int),
         ("adjoint_jacobian", C.c_int),
         ("adjoint_fd_step", C.c_double),
+        ("adjoint_precision", C.c_int),
     ]
 
 

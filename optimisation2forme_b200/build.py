@@ -90,6 +90,10 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         learned = src.stem.startswith("mlp")
         fmad = "-fmad=true" if src.stem.endswith("_f32") or learned else "-fmad=false"
         extra = [f"-I{_cutlass_include()}"] if learned else []
+        if src.stem.endswith("_f32"):
+            # FP32 residual: approximate division and square root, FP32
+            # denormals flushed (FP64 code in the unit is unaffected)
+            extra += ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
         if force or _stale(obj, _deps(src)):
             jobs.append([nvcc, *ARCH, "-O3", "-std=c++17", "-lineinfo", fmad, "--expt-relaxed-constexpr",
                          "-Xcompiler", "-fPIC,-ffp-contract=off", *inc, *extra, "-c", str(src), "-o", str(obj)])

@@ -203,10 +203,16 @@ __global__ void __launch_bounds__(128) k_ilu_factor(const int32_t* __restrict__ 
 constexpr int kSweepBlock = 128;
 constexpr long long kSweepSpinLimit = 1ll << 22;
 
-__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int* p) {
   unsigned int v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 __device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
@@ -260,14 +266,26 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
       }
     }
   }
+  // The row's blocks (and D^-1 for the backward sweep) do not depend on the
+  // flags: bring them towards L1 while the row waits.
+  if (active) {
+    const char* rowp = reinterpret_cast<const char*>(ilu.A + (int64_t)i * 80);
+#pragma unroll
+    for (int b = 0; b < 5; ++b) prefetch_l1(rowp + 128 * b);
+    if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)i * 16);
+  }
   bool done = !active;
   long long spins = 0;
   while (__any_sync(kFull, !done)) {
     if (done) continue;
+    // All flags polled at once (relaxed loads, in flight together); once
+    // every one carries this launch's value, the fence turns the reads into
+    // an acquire of the producers' released stores of y.
     bool ready = true;
     for (int d = 0; d < ndep; ++d)
-      if (ld_acquire_u32(flag + dep[d]) != want) ready = false;
+      if (ld_relaxed_u32(flag + dep[d]) != want) ready = false;
     if (ready) {
+      fence_acq_rel_gpu();
       const double* row = ilu.A + (int64_t)i * 80;
       Vec4<double> acc = kForward ? r[i] : ldcg4(y + i);
       for (int d = 0; d < ndep; ++d) {

@@ -75,10 +75,12 @@ O2F_QDIV_FN double qdiv_flag(double a, double b, double y, bool& ok) {
   return fma(r1, y, q1);
 }
 
-// FP32 instantiations (the mixed-precision path) keep the plain division.
-O2F_QDIV_FN float recip_for_div(float b) { return b; }
-O2F_QDIV_FN float recip_for_div(float b, float) { return b; }
-O2F_QDIV_FN float qdiv(float a, float b, float) { return a / b; }
-O2F_QDIV_FN float qdiv_flag(float a, float b, float, bool&) { return a / b; }
+// FP32 instantiations (the mixed-precision path, which is not bit-exact by
+// design): one reciprocal per divisor, each quotient a multiplication
+// (within 1.5 ulp of a/b).
+O2F_QDIV_FN float recip_for_div(float b) { return 1.0f / b; }
+O2F_QDIV_FN float recip_for_div(float, float inv_b) { return inv_b; }
+O2F_QDIV_FN float qdiv(float a, float, float y) { return a * y; }
+O2F_QDIV_FN float qdiv_flag(float a, float, float y, bool&) { return a * y; }
 
 }  // namespace o2f

@@ -47,6 +47,8 @@ void validate_params(const o2f_params& p) {
   if (p.limiter != O2F_LIMITER_VENKAT && p.limiter != O2F_LIMITER_BARTH_JESPERSEN)
     throw Error(O2F_ERR_ARG, "unknown limiter");
   if (p.precision != O2F_PREC_F64 && p.precision != O2F_PREC_F32) throw Error(O2F_ERR_ARG, "unknown precision");
+  if (p.adjoint_precision != O2F_PREC_F64 && p.adjoint_precision != O2F_PREC_F32)
+    throw Error(O2F_ERR_ARG, "unknown adjoint_precision");
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
   if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
@@ -98,6 +100,11 @@ Solver::Solver(const o2f_mesh_desc& desc, const o2f_params& p, cudaStream_t stre
   if (hm_.nc >= (int64_t(1) << 30) || hm_.ne >= (int64_t(1) << 30)) throw Error(O2F_ERR_MESH, "mesh too large");
   O2F_CUDA(cudaEventCreate(&ev0_));
   O2F_CUDA(cudaEventCreate(&ev1_));
+  // Pinned mailbox of the device-driven loops (step / Krylov state), kept
+  // for the context's life: no pinned allocation or free during a solve,
+  // whose implicit synchronisation could disturb another thread's stream
+  // capture.
+  O2F_CUDA(cudaMallocHost(&mailbox_, std::max(sizeof(StepState), sizeof(KrylovState))));
   params_ = p;
   min_h_ = min_cell_h(hm_);
   upload_mesh();
@@ -110,6 +117,7 @@ Solver::~Solver() {
   if (stream_) cudaStreamSynchronize(stream_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (mailbox_) cudaFreeHost(mailbox_);
   if (own_stream_ && stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1050,8 +1058,7 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
   }
   O2F_CUDA(cudaStreamEndCapture(stream_, &graph));
   O2F_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-  StepState* host_st = nullptr;
-  O2F_CUDA(cudaMallocHost(&host_st, sizeof(StepState)));
+  StepState* host_st = static_cast<StepState*>(mailbox_);
   int64_t launched = 0;
   try {
     while (true) {
@@ -1067,13 +1074,11 @@ void Solver::rk3_run(int64_t max_steps, double drop_tol, double* history, int64_
   } catch (...) {
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
-    cudaFreeHost(host_st);
     throw;
   }
   const StepState fin = *host_st;
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
-  cudaFreeHost(host_st);
   if (history && fin.step > 0)
     O2F_CUDA(cudaMemcpy(history, hist_dev_, std::min<int64_t>(fin.step, max_steps) * sizeof(double),
                         cudaMemcpyDeviceToHost));
@@ -1108,7 +1113,7 @@ void Solver::build_jt_blocks() {
   k_jt_blocks<<<(int)((topo_.ne + 127) / 128), 128, 0, stream_>>>(topo_.ne, geom_, topo_.ebc, work_.eL, work_.eR,
                                                                    phys_, 1e-6, blk_);
   O2F_CUDA(cudaGetLastError());
-  if (f32()) f32_blocks();
+  if (mixed_adjoint()) f32_blocks();
   blk_valid_ = true;
 }
 
@@ -1348,7 +1353,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     if (precond) ilu_apply(p_, ph, kgate);
     if (full)
       k_bicg_fjt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, ph, v_, r0_, part_, ks_);
-    else if (f32())  // FP32 blocks; restarts take the true residual with the FP64 operator
+    else if (mixed_adjoint())  // FP32 blocks; restarts take the true residual with the FP64 operator
       k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, ph, v_, r0_,
                                                     part_, ks_);
     else
@@ -1359,7 +1364,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     if (precond) ilu_apply(s_, sh, kgate);
     if (full)
       k_bicg_fjt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, sh, s_, t_, part_, ks_);
-    else if (f32())
+    else if (mixed_adjoint())
       k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, sh, s_, t_,
                                                     part_, ks_);
     else
@@ -1372,8 +1377,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   }
   O2F_CUDA(cudaStreamEndCapture(stream_, &graph));
   O2F_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-  KrylovState* hks = nullptr;
-  O2F_CUDA(cudaMallocHost(&hks, sizeof(KrylovState)));
+  KrylovState* hks = static_cast<KrylovState*>(mailbox_);
   int err = O2F_OK;
   std::string msg;
   try {
@@ -1434,12 +1438,10 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   } catch (...) {
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
-    cudaFreeHost(hks);
     throw;
   }
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
-  cudaFreeHost(hks);
   have_lambda_ = true;
   if (iters) *iters = total;
   if (relres_out) *relres_out = relres;

@@ -141,6 +141,8 @@ class Solver {
   Work<double> alloc_work();
   // mixed precision (solver_f32.cu)
   bool f32() const { return params_.precision == O2F_PREC_F32; }
+  // FP32 Jacobian blocks in the Krylov products (FP64 true residuals)
+  bool mixed_adjoint() const { return f32() || params_.adjoint_precision == O2F_PREC_F32; }
   Work<float> alloc_work_f32();
   void ensure_f32();
   void f32_state_sync();
@@ -231,6 +233,7 @@ class Solver {
   double last_residual_ms_ = 0.0;
   int64_t launches_ = 0;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  void* mailbox_ = nullptr;  // pinned host copy of StepState / KrylovState
 };
 
 }  // namespace o2f

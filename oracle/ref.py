@@ -28,6 +28,19 @@ def available() -> bool:
     return EXE_EXACT.exists() and EXE_ADAPTER.exists()
 
 
+def stale() -> bool:
+    """True when a built binary is missing or older than a source it is built
+    from here (the harness, the adapter check, the adapter and the C ABI
+    header it compiles in)."""
+    if not available():
+        return True
+    root = HERE.parent
+    deps = [HERE / "ref_harness.cpp", HERE / "adapter_check.cpp", HERE / "build_ref.sh", root / "include" / "o2f.h",
+            root / "optimisation2forme_b200" / "adapters" / "navier_stokes_o2f.cpp"]
+    t = min(EXE_EXACT.stat().st_mtime, EXE_ADAPTER.stat().st_mtime)
+    return any(d.exists() and d.stat().st_mtime > t for d in deps)
+
+
 def build() -> bool:
     """Compile the reference from its sources when they are present."""
     if (REF_DIR / "src" / "advection.cpp").exists():

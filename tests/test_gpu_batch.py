@@ -188,3 +188,37 @@ def test_batch_rejects_mixed_precisions():
             Solver(_params(precision="fp32", **pk1), desc=desc_of(small_mesh(**mk1))) as b:
         with pytest.raises(O2FError):
             Batch([a, b])
+
+
+def test_concurrent_adjoints_on_own_streams_equal_sequential_ones():
+    """Adjoint solves and shape gradients of several contexts run at once
+    from host threads, each context on its own stream (as the fast path runs
+    its candidates' adjoints): every result equals the same context's solve
+    run alone, bit for bit."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from optimisation2forme_b200 import Solver
+    streams = [torch.cuda.Stream() for _ in CANDIDATES]
+    ctxs = [Solver(_params(adjoint_precision="fp32", **pk), desc=desc_of(small_mesh(**mk)), stream=st.cuda_stream)
+            for (mk, pk), st in zip(CANDIDATES, streams)]
+
+    def run(s):
+        s.initialize_freestream()
+        s.time_loop(40)
+        a = s.solve_adjoint_system(0.1, tol=1e-9, max_iter=5000, restart=500)
+        g = s.compute_shape_gradient(["m", "p", "t"], Solver.shape_params(), beta=0.1)
+        return a["lambda"], a["iters"], g
+
+    try:
+        alone = [run(s) for s in ctxs]
+        with ThreadPoolExecutor(max_workers=len(ctxs)) as ex:
+            together = list(ex.map(run, ctxs))
+        for (l0, i0, g0), (l1, i1, g1) in zip(alone, together):
+            assert i0 == i1
+            assert bits_equal(l0, l1)
+            assert bits_equal(g0, g1)
+    finally:
+        for s in ctxs:
+            s.close()

@@ -131,3 +131,36 @@ def test_mixed_jt_product_uses_fp32_blocks():
         d = np.linalg.norm(ya - yb) / np.linalg.norm(ya)
         print(f"\nmixed: J^T product {d:.2e}")
         assert 0.0 < d <= 1e-6  # FP32-rounded blocks: different, within FP32 rounding
+
+
+TOL_DJ_MIXED_ADJOINT = 1e-4  # the bar; measured far below it (FP64 true residual to 1e-10)
+
+
+def test_mixed_adjoint_of_an_fp64_state_meets_the_dj_bar():
+    """adjoint_precision = fp32 in an FP64 context (the fast path's adjoint):
+    FP32 Jacobian blocks in the BiCGSTAB products, every restart's true
+    residual with the FP64 operator.  Same state and linearisation as the
+    FP64 path, so lambda and dJ/dshape agree with the oracle's FP64 gradient
+    about its direct-solve adjoint within the 1e-4 bar."""
+    import scipy.sparse.linalg as sla
+    from optimisation2forme_b200 import HostMesh, Solver
+    m = _mesh()
+    p64 = _params()
+    hm = HostMesh(desc=desc_of(m))
+    o = cpu.Oracle(hm, p64)
+    sh = Solver.shape_params(["m", "p", "t", "pos_x"], [0.02, 0.4, 0.12, 0.355])
+    with Solver(dataclasses.replace(p64, adjoint_precision="fp32"), desc=desc_of(m)) as b:
+        b.initialize_freestream()
+        b.time_loop(300)
+        U = b.get_state()
+        r = o.residual(U)
+        lam_o = sla.spsolve(assemble_jt(o, hm, r["edge_LR"]).tocsc(), o.rhs(r["edge_LR"], 0.1))
+        g_o = o.shape_gradient(U, lam_o, sh, [0, 1, 2], 0.1)
+        b.compute_residual()
+        res = b.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=5000)
+        g = b.compute_shape_gradient(["m", "p", "t"], sh, beta=0.1)
+        dlam = np.linalg.norm(res["lambda"] - lam_o) / np.linalg.norm(lam_o)
+        dg = np.abs(g - g_o) / np.abs(g_o).max()
+        print(f"\nmixed adjoint, FP64 state: iters {res['iters']} relres {res['relres']:.2e} lambda {dlam:.2e} dJ {dg}")
+        assert res["relres"] <= 1e-10
+        assert np.all(dg <= TOL_DJ_MIXED_ADJOINT)

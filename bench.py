@@ -205,6 +205,39 @@ def roofline_2m(args, peaks) -> dict:
     return out
 
 
+def run_kernels(args) -> dict:
+    """The residual kernels alone (FP64 and FP32) on the transonic NACA 0012
+    mesh named by --mesh ("large": 2.0M cells, "medium": 1.0M cells) about a
+    state --rk-steps RK3 steps from the freestream: CUDA-event times per
+    launch and the byte models.  The command the ncu summaries in profiles/
+    are taken from."""
+    from optimisation2forme_b200 import SimulationParams, Solver, mesh_desc
+    from optimisation2forme_b200.meshgen import config_mesh, naca_ogrid
+    spec, flow = config_mesh(args.mesh)
+    mesh = naca_ogrid(spec)
+    nnz = int(mesh["cell_offsets"][-1])
+    peaks = load_peaks()
+    out = {"mesh": args.mesh}
+    for prec, w in (("fp64", 8), ("fp32", 4)):
+        p = SimulationParams(viscosity=1.8e-5, inflow_velocity=flow["mach"], aoa_deg=flow["aoa"], cfl_number=0.3,
+                             final_time=1e30, limiter_k=5.0, dt_mode="thermal", verbosity=0, precision=prec)
+        with Solver(p, desc=mesh_desc(mesh["node_xy"], mesh["segments"], mesh["segment_bc"], mesh["cell_offsets"],
+                                      mesh["cell_nodes"])) as s:
+            s.initialize_freestream()
+            s.time_loop(args.rk_steps)
+            prof = s.profile_kernels(args.profile_reps)
+            nc, ne, nv = s.n_cells, s.n_edges, s.n_vertices
+        kb = kernel_bytes(nc, ne, nv, nnz, w)
+        res_ms = sum(prof[k] for k in RESIDUAL_KERNELS)
+        out[prec] = {"kernel_ms": {k: round(v, 5) for k, v in prof.items()},
+                     "kernel_bytes": {k: kb[k] for k in RESIDUAL_KERNELS},
+                     "residual_ms": round(res_ms, 4),
+                     "residual_frac": round(residual_bytes(nc, ne, nv, nnz, w) / (res_ms / 1e3) / 1e9 /
+                                            peaks["hbm_gbs"], 4)}
+        out["cells"] = nc
+    return out
+
+
 def roofline_entry(roof: dict, peaks: dict) -> dict:
     """`roofline` of the line: the whole FP64 residual on the 2.0M-cell mesh
     (compulsory single-pass bytes / the five kernels' summed time), with the
@@ -671,7 +704,8 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="o2f", choices=["o2f", "reference"])
-    ap.add_argument("--workload", default="candidates", choices=["candidates", "large"])
+    ap.add_argument("--workload", default="candidates", choices=["candidates", "large", "kernels"])
+    ap.add_argument("--mesh", default="large", choices=["large", "medium"], help="mesh of --workload kernels")
     ap.add_argument("--candidates", type=int, default=16)
     ap.add_argument("--cells-lo", type=float, default=50_000)
     ap.add_argument("--cells-hi", type=float, default=400_000)
@@ -709,6 +743,8 @@ def main() -> int:
             line = run_reference(args, rank, world)
         elif args.workload == "large":
             line = run_large(args, rank, world)
+        elif args.workload == "kernels":
+            line = run_kernels(args) if rank == 0 else None
         else:
             line = run_candidates(args, rank, world)
     finally:

@@ -102,13 +102,11 @@ struct Phys {
 
 // Block ILU(0) preconditioner of the adjoint operator (see ilu.cuh).
 // State of one sync-free triangular sweep (one per direction): warps take
-// 32-row chunks in ILU order from `claim`; the last warp to finish resets
-// claim/done and advances `epoch`, so a row is ready in the current launch
-// when its flag equals epoch + 1.
+// 32-row chunks in sweep order from `claim`; the last warp to finish resets
+// claim/done for the next launch.
 struct SweepSync {
   unsigned int claim;
   unsigned int done;
-  unsigned int epoch;
   int err;  // a dependency wait ran past its limit (the sweep's result is invalid)
 };
 
@@ -121,7 +119,7 @@ struct IluDev {
   double* A;          // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
   double* Dinv;       // [nc*16]
   int32_t* lo_cells;  // [nc] factorization levels, concatenated (offsets kept on the host)
-  uint32_t* flag;     // [2*nc] ready flags of the forward, then the backward sweep
+  Vec4<double>* tmp;  // [nc] forward sweep's output / backward sweep's input (empty between applications)
   SweepSync* sync;    // [2] forward, backward
   int n_lo;
   long long spin_limit;  // polls a sweep row waits before it gives up (error status)

@@ -194,63 +194,77 @@ __global__ void __launch_bounds__(128) k_ilu_factor(const int32_t* __restrict__ 
 // 32-row chunk are mostly independent.  Each warp takes one chunk from a
 // counter, so every chunk before it already belongs to a running warp and
 // the earliest unfinished row always has its dependencies done: the waits
-// cannot deadlock.  A row waits on the
-// ready flags of its lower (forward) or upper (backward) neighbours, solves
-// its 4-vector and releases its own flag.  Waits are bounded: past
-// ilu.spin_limit polls (default kSweepSpinLimit) the warp records sync->err
-// and stops waiting, and
-// every other waiting row gives up once it sees the error.
+// cannot deadlock.
+//
+// The solved values are their own ready signals: every output slot holds
+// the sentinel bit pattern kSweepEmpty until its row writes the solution,
+// and a waiting row polls the 8-byte words of its dependencies' slots
+// (relaxed loads at GPU scope, single-copy atomic per word) until none is
+// the sentinel, so a level costs one L2 round trip and no fence.  The
+// forward sweep writes into ilu.tmp and resets the backward sweep's output
+// to the sentinel; the backward sweep reads ilu.tmp and resets it after
+// reading, so both buffers are empty again for the next application.  A
+// computed NaN is stored as the canonical NaN, never as the sentinel.
+//
+// Waits are bounded: past ilu.spin_limit polls (default kSweepSpinLimit) the
+// warp records sync->err and stops waiting, and every other waiting row
+// gives up once it sees the error; the host turns it into an error status.
 constexpr int kSweepBlock = 128;
 constexpr long long kSweepSpinLimit = 1ll << 22;
-
-__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int* p) {
-  unsigned int v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+constexpr unsigned long long kSweepEmpty = 0x7ff4f11ed5eed000ull;  // a NaN no arithmetic produces
 
 __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
-__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const void* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
 }
 
-__device__ __forceinline__ Vec4<double> ldcg4(const Vec4<double>* p) {
-  const double2* q = reinterpret_cast<const double2*>(p);
-  const double2 a = __ldcg(q), b = __ldcg(q + 1);
-  return Vec4<double>{a.x, a.y, b.x, b.y};
+__device__ __forceinline__ void st_relaxed_u64(void* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// kForward: y_i = r_i - sum_{k lower} L_ik y_k.
-// backward: z_i = D_i^{-1} (y_i - sum_{j upper} U_ij z_j), in place (y == z).
+__device__ __forceinline__ unsigned long long sweep_bits(double x) {
+  return x != x ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(x);
+}
+
+__device__ __forceinline__ void store_empty(Vec4<double>* p) {
+  unsigned long long* q = reinterpret_cast<unsigned long long*>(p);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) st_relaxed_u64(q + k, kSweepEmpty);
+}
+
+// Fill a sweep buffer with the sentinel (set-up of ilu.tmp).
+__global__ void k_ilu_empty(int64_t n, Vec4<double>* y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) store_empty(y + i);
+}
+
+// kForward: tmp_i = r_i - sum_{k lower} L_ik tmp_k; z_i <- empty.
+// backward: z_i = D_i^{-1} (tmp_i - sum_{j upper} U_ij z_j); tmp_i <- empty.
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, const Vec4<double>* r,
-                                                           Vec4<double>* y, const int* gate) {
+                                                           Vec4<double>* z, const int* gate) {
   if (gated(gate)) return;
   constexpr unsigned int kFull = 0xffffffffu;
   SweepSync* sync = ilu.sync + (kForward ? 0 : 1);
-  unsigned int* flag = ilu.flag + (kForward ? 0 : ilu.nc);
+  Vec4<double>* out = kForward ? ilu.tmp : z;  // slots this sweep fills (empty on entry)
   const int lane = threadIdx.x & 31;
   const unsigned int nchunks = (unsigned int)(n + 31) / 32u;
   // Surplus warps of the last block leave before claiming: exactly nchunks
   // claims per launch, so the reset below runs after the last claim.
   if (blockIdx.x * (unsigned int)(kSweepBlock / 32) + (threadIdx.x >> 5) >= nchunks) return;
-  unsigned int chunk = 0, epoch = 0;
-  if (lane == 0) {
-    chunk = atomicAdd(&sync->claim, 1u);
-    epoch = *reinterpret_cast<volatile unsigned int*>(&sync->epoch);
-  }
+  unsigned int chunk = 0;
+  if (lane == 0) chunk = atomicAdd(&sync->claim, 1u);
   chunk = __shfl_sync(kFull, chunk, 0);
-  epoch = __shfl_sync(kFull, epoch, 0);
-  const unsigned int want = epoch + 1u;
   const int64_t nc = ilu.nc;
   const int p = (int)chunk * 32 + lane;
   const bool active = p < n;
   int i = 0, dep[4], ndep = 0, slot[4];
+  Vec4<double> own{};
   if (active) {
     i = ilu.sweep[kForward ? p : (int64_t)n + p];
     const int pi = ilu.pos[i];
@@ -265,32 +279,43 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
         ++ndep;
       }
     }
-  }
-  // The row's blocks (and D^-1 for the backward sweep) do not depend on the
-  // flags: bring them towards L1 while the row waits.
-  if (active) {
+    // The row's blocks (and D^-1 backward) do not depend on the waits:
+    // bring them towards L1 first.
     const char* rowp = reinterpret_cast<const char*>(ilu.A + (int64_t)i * 80);
 #pragma unroll
     for (int b = 0; b < 5; ++b) prefetch_l1(rowp + 128 * b);
     if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)i * 16);
+    if (kForward) {
+      own = r[i];
+      store_empty(z + i);  // the backward sweep's slot
+    } else {
+      const double2* t = reinterpret_cast<const double2*>(ilu.tmp + i);
+      const double2 a = __ldcg(t), b = __ldcg(t + 1);
+      own = Vec4<double>{a.x, a.y, b.x, b.y};
+      store_empty(ilu.tmp + i);  // empty again for the next forward sweep
+    }
   }
   bool done = !active;
   long long spins = 0;
   while (__any_sync(kFull, !done)) {
     if (done) continue;
-    // All flags polled at once (relaxed loads, in flight together); once
-    // every one carries this launch's value, the fence turns the reads into
-    // an acquire of the producers' released stores of y.
     bool ready = true;
-    for (int d = 0; d < ndep; ++d)
-      if (ld_relaxed_u32(flag + dep[d]) != want) ready = false;
+    unsigned long long w[4][4];
+    for (int d = 0; d < ndep; ++d) {
+      const unsigned long long* q = reinterpret_cast<const unsigned long long*>(out + dep[d]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        w[d][k] = ld_relaxed_u64(q + k);
+        if (w[d][k] == kSweepEmpty) ready = false;
+      }
+    }
     if (ready) {
-      fence_acq_rel_gpu();
       const double* row = ilu.A + (int64_t)i * 80;
-      Vec4<double> acc = kForward ? r[i] : ldcg4(y + i);
+      Vec4<double> acc = own;
       for (int d = 0; d < ndep; ++d) {
         const double* Bk = row + 16 * (1 + slot[d]);
-        const Vec4<double> v = ldcg4(y + dep[d]);
+        const Vec4<double> v{__longlong_as_double((long long)w[d][0]), __longlong_as_double((long long)w[d][1]),
+                             __longlong_as_double((long long)w[d][2]), __longlong_as_double((long long)w[d][3])};
         acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
         acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
         acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
@@ -298,16 +323,20 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
       }
       if (!kForward) {
         const double* D = ilu.Dinv + (int64_t)i * 16;
-        Vec4<double> out;
-        out.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
-        out.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
-        out.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
-        out.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
-        acc = out;
+        Vec4<double> o4;
+        o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
+        o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
+        o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
+        o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
+        acc = o4;
       }
-      y[i] = acc;
-      if (!kForward || i != ilu.stall_row)
-        st_release_u32(flag + i, want);  // orders the store of y[i] before the flag
+      if (!kForward || i != ilu.stall_row) {
+        unsigned long long* q = reinterpret_cast<unsigned long long*>(out + i);
+        st_relaxed_u64(q, sweep_bits(acc.a));
+        st_relaxed_u64(q + 1, sweep_bits(acc.b));
+        st_relaxed_u64(q + 2, sweep_bits(acc.c));
+        st_relaxed_u64(q + 3, sweep_bits(acc.d));
+      }
       done = true;
     } else if ((++spins & 63) == 0) {
       if (spins > ilu.spin_limit) {
@@ -326,7 +355,6 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
       sync->claim = 0;
       sync->done = 0;
       __threadfence();
-      atomicAdd(&sync->epoch, 1u);
     }
   }
 }

@@ -677,7 +677,7 @@ void Solver::ilu_factor() {
     ilu_.order = arena_.alloc<int32_t>(nc);
     ilu_.sweep = arena_.alloc<int32_t>(2 * nc);
     ilu_.lo_cells = arena_.alloc<int32_t>(nc);
-    ilu_.flag = arena_.alloc<uint32_t>(2 * nc);
+    ilu_.tmp = arena_.alloc<Vec4<double>>(nc);
     ilu_.sync = arena_.alloc<SweepSync>(2);
     ilu_status_ = arena_.alloc<int>(1);
     phat_ = arena_.alloc<Vec4<double>>(nc);
@@ -687,7 +687,7 @@ void Solver::ilu_factor() {
     h2d(ilu_.order, ilu_order_h_, s);
     h2d(ilu_.sweep, ilu_sweep_h_, s);
     h2d(ilu_.lo_cells, lo_cells_h_, s);
-    O2F_CUDA(cudaMemsetAsync(ilu_.flag, 0, 2 * nc * sizeof(uint32_t), s));
+    k_ilu_empty<<<grid(nc), kBlock, 0, s>>>(nc, ilu_.tmp);
     O2F_CUDA(cudaMemsetAsync(ilu_.sync, 0, 2 * sizeof(SweepSync), s));
     sync();
     ilu_alloc_ = true;
@@ -710,7 +710,7 @@ void Solver::ilu_factor() {
   if (st) throw Error(O2F_ERR_BREAKDOWN, "singular block in the ILU(0) factorization");
 }
 
-// z = M^{-1} r: forward levels into z, backward levels in place.
+// z = M^{-1} r: the forward sweep into ilu_.tmp, the backward sweep into z.
 // z = U^{-1} L^{-1} r: one sync-free launch per triangle, one warp per
 // 32-row chunk (surplus warps of the last block exit without claiming).
 void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) {
@@ -719,13 +719,13 @@ void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) 
   const int chunks = (n + 31) / 32;
   const int warps_per_block = kSweepBlock / 32;
   const int blocks = (chunks + warps_per_block - 1) / warps_per_block;
-  k_ilu_sweep<true><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, r, z, gate);
-  k_ilu_sweep<false><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, z, z, gate);
+  k_ilu_sweep<true><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, r, z, gate);  // r -> ilu_.tmp
+  k_ilu_sweep<false><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, nullptr, z, gate);  // ilu_.tmp -> z
 }
 
 // Test hook: the next solves run their sweeps with `spin_limit` polls per
-// wait, and with `stall` the first row of the forward order never releases
-// its flag, so the rows that depend on it wait out their limit (no fault:
+// wait, and with `stall` the first row of the forward order never writes its
+// value, so the rows that depend on it wait out their limit (no fault:
 // every wait is bounded).  spin_limit <= 0 and stall = 0 restore the
 // defaults.  Takes effect for the solves that start after the call.
 void Solver::debug_ilu_stall(int stall, long long spin_limit) {

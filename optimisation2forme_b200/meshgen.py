@@ -204,6 +204,7 @@ def config_mesh(name: str, seed: int = 0) -> tuple[OGridSpec, dict]:
     * ``small``  -- NACA 2412, ~20k triangles, M=0.6, AoA=2 deg, Re=5000.
     * ``large``  -- NACA 0012, ~2M triangles, first cell 1e-4 chord, growth
       1.1, M=0.85, AoA=1.25 deg, Re=1e4 (the transonic case).
+    * ``medium`` -- the same case at ~1M triangles (kernel profiles).
     * ``mixed``  -- ~500k triangles, seeded (m, p, t, M, AoA).
     """
     if name == "small":
@@ -212,6 +213,10 @@ def config_mesh(name: str, seed: int = 0) -> tuple[OGridSpec, dict]:
         flow = dict(mach=0.6, aoa=2.0, reynolds=5000.0)
     elif name == "large":
         spec = OGridSpec(m=0.0, p=0.4, t=0.12, n_surface=1400, n_layers=715, first_height=1e-4, growth=1.1,
+                         seed=seed)
+        flow = dict(mach=0.85, aoa=1.25, reynolds=1e4)
+    elif name == "medium":
+        spec = OGridSpec(m=0.0, p=0.4, t=0.12, n_surface=1000, n_layers=505, first_height=1e-4, growth=1.1,
                          seed=seed)
         flow = dict(mach=0.85, aoa=1.25, reynolds=1e4)
     elif name == "mixed":

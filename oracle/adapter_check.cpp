@@ -49,6 +49,12 @@ using namespace navier_stokes;
 
 namespace {
 
+// Progress on stderr, so that a failing run shows how far it got.
+void phase(const char* what) {
+  std::fprintf(stderr, "o2f_adapter_check: %s\n", what);
+  std::fflush(stderr);
+}
+
 // Same bits, except that +0.0 and -0.0 count as equal (see the adapter's
 // computeAdvectionTerm).
 bool same(double a, double b) {
@@ -100,13 +106,17 @@ int main(int argc, char** argv) {
     initialize_flow_field(ref, params);
     loadCellStates(ref, params);
     Mesh ada = ref;
+    phase("reference mesh and state loaded");
 
     // advection + diffusion, as Simulator::rk3_substep calls them
     computeAdvectionTerm(ref, params);
+    phase("reference advection done");
     o2f_adapter::computeAdvectionTerm(ada, params);
+    phase("adapter advection done");
     const long adv_cells = count_cells(ref, ada, true), adv_edges = count_edges(ref, ada, false);
     computeDiffusionTerm(ref, params);
     o2f_adapter::computeDiffusionTerm(ada, params);
+    phase("diffusion done");
     const long res_cells = count_cells(ref, ada, true), res_edges = count_edges(ref, ada, true);
 
     // computeResidual and the forces on fresh copies
@@ -114,6 +124,7 @@ int main(int argc, char** argv) {
     std::vector<double> a0, a1, a2, a3, b0, b1, b2, b3;
     computeResidual(ref2, params, a0, a1, a2, a3);
     o2f_adapter::computeResidual(ada2, params, b0, b1, b2, b3);
+    phase("computeResidual done");
     long cr = 0;
     for (size_t i = 0; i < a0.size(); ++i)
       cr += !same(a0[i], b0[i]) + !same(a1[i], b1[i]) + !same(a2[i], b2[i]) + !same(a3[i], b3[i]);
@@ -124,6 +135,7 @@ int main(int argc, char** argv) {
     const double force_err = std::max(std::fabs(CLr - CLa) / std::max(std::fabs(CLr), 1e-300),
                                       std::fabs(CDr - CDa) / std::max(std::fabs(CDr), 1e-300));
 
+    phase("forces done");
     // compute_hllc_flux on every edge's interface states
     long hllc = 0;
     for (auto& e : ref2.edges) {
@@ -133,6 +145,7 @@ int main(int argc, char** argv) {
       for (int k = 0; k < 4; ++k) hllc += !same(f[k], g[k]);
     }
 
+    phase("hllc done");
     // the boundary functions for every code on a cell's state
     long bc = 0;
     const char codes[] = {'i', 'o', 'f', 'w', '\0', 'x'};

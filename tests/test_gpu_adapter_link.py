@@ -28,7 +28,7 @@ def test_adapter_matches_the_reference_bit_for_bit(golden_dir, tmp_path):
     r = subprocess.run([str(ref.EXE_ADAPTER), str(cfg)], capture_output=True, text=True, cwd=tmp_path,
                        env={**os.environ, "OMP_NUM_THREADS": "1"}, timeout=600)
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
-    assert lines, r.stdout + r.stderr
+    assert lines, f"exit status {r.returncode}; stdout: {r.stdout!r}; stderr: {r.stderr!r}"
     out = json.loads(lines[-1])
     print("\nadapter vs reference:", out)
     assert out["cells"] == 25274

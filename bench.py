@@ -422,7 +422,7 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
 
     # -- fast arm: one batched time loop, then each candidate's adjoint from
     # the network's prediction (mixed-precision BiCGSTAB, FP64 refinement)
-    def fast_pass(states=None, serial=False):
+    def fast_pass(states=None, serial=False, warm=True):
         for i, s in enumerate(fast):
             if states is None:
                 s.initialize_freestream()
@@ -434,7 +434,7 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
             raise RuntimeError(f"fast time loop failed for candidates {bad}")
         # the network's predictions (one network: one call at a time), then
         # every candidate's adjoint and gradient at once
-        guesses = [ws.guess(s, c) if ws else None for s, c in zip(fast, cands)]
+        guesses = [ws.guess(s, c) if ws and warm else None for s, c in zip(fast, cands)]
         work = [lambda k=k: adjoint_and_gradient(fast[k], cands[k], guesses[k]) for k in range(len(cands))]
         if serial:  # the first pass allocates each context's adjoint buffers
             return [w() for w in work]
@@ -446,6 +446,8 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
     fast_out = fast_pass(serial=True)
     for _ in range(max(args.warmup - 1, 0)):
         fast_out = fast_pass()
+    # the same pass without the network's guesses (untimed): what it saves
+    cold_it = [o["iters"] for o in fast_pass(warm=False)] if ws else None
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -531,6 +533,7 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
             "target_5x_met": value / plain_value >= 5.0 and max(errs) <= DJ_BAR,
             "adjoint_converged_all": converged, "adjoint_tol": ADJ_TOL,
             "adjoint_iters_fast": fast_it, "adjoint_iters_plain": plain_it,
+            "adjoint_iters_fast_without_warm_start": cold_it,
             "warm_start": None if ws is None else {"train_candidates": args.train_candidates,
                                                     "fields": ws.n_fields, "points": ws.n_points,
                                                     "adam_steps": args.train_steps,
@@ -714,7 +717,7 @@ def main() -> int:
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--fast-precision", default="fp64", choices=["fp32", "fp64"])
     ap.add_argument("--no-warm-start", action="store_true")
-    ap.add_argument("--train-candidates", type=int, default=16)
+    ap.add_argument("--train-candidates", type=int, default=8)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--plain-warmup", type=int, default=1)

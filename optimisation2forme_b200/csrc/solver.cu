@@ -884,6 +884,7 @@ void Solver::residual(double* R_ref) {
 }
 
 void Solver::profile_kernels(int reps, double* ms_out) {
+  NvtxRange nvtx_("o2f profile_kernels");
   if (reps <= 0) throw Error(O2F_ERR_ARG, "reps must be positive");
   const Topo& t = topo_;
   const Geom<double>& g = geom_;

@@ -121,7 +121,9 @@ int main(int argc, char** argv) {
 
     // computeResidual and the forces on fresh copies
     Mesh ref2 = ref, ada2 = ref;
-    std::vector<double> a0, a1, a2, a3, b0, b1, b2, b3;
+    // the reference writes into vectors of the cell count (it does not resize them)
+    const size_t nc = ref.cells.size();
+    std::vector<double> a0(nc), a1(nc), a2(nc), a3(nc), b0, b1, b2, b3;
     computeResidual(ref2, params, a0, a1, a2, a3);
     o2f_adapter::computeResidual(ada2, params, b0, b1, b2, b3);
     phase("computeResidual done");

@@ -102,11 +102,11 @@ struct Phys {
 
 // Block ILU(0) preconditioner of the adjoint operator (see ilu.cuh).
 // State of one sync-free triangular sweep (one per direction): warps take
-// 32-row chunks in sweep order from `claim`; the last warp to finish resets
+// 32-row chunks in sweep order from `claim`; the last warp to leave resets
 // claim/done for the next launch.
 struct SweepSync {
   unsigned int claim;
-  unsigned int done;
+  unsigned int done;  // warps of the launch that have left
   int err;  // a dependency wait ran past its limit (the sweep's result is invalid)
 };
 

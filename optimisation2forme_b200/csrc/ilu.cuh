@@ -191,10 +191,8 @@ __global__ void __launch_bounds__(128) k_ilu_factor(const int32_t* __restrict__ 
 // Sync-free triangular sweeps (one launch per triangle).  Rows are processed
 // in a level order of the triangle's dependency graph (ilu.sweep: forward
 // levels, then backward levels), a topological order, so the rows of one
-// 32-row chunk are mostly independent.  Each warp takes one chunk from a
-// counter, so every chunk before it already belongs to a running warp and
-// the earliest unfinished row always has its dependencies done: the waits
-// cannot deadlock.
+// 32-row chunk are mostly independent.  Warps take chunks from a counter
+// (see k_ilu_sweep for why the waits cannot deadlock).
 //
 // The solved values are their own ready signals: every output slot holds
 // the sentinel bit pattern kSweepEmpty until its row writes the solution,
@@ -245,6 +243,15 @@ __global__ void k_ilu_empty(int64_t n, Vec4<double>* y) {
 
 // kForward: tmp_i = r_i - sum_{k lower} L_ik tmp_k; z_i <- empty.
 // backward: z_i = D_i^{-1} (tmp_i - sum_{j upper} U_ij z_j); tmp_i <- empty.
+// A small grid of persistent warps (ilu_sweep_blocks): each warp claims the
+// next 32-row chunk, solves it, and claims again, so only the warps near the
+// front of the dependency levels poll -- a launch of one warp per chunk kept
+// thousands of warps polling and saturated the load path.  Claims are in
+// order and a warp claims again only after finishing its chunk, so every
+// claimed chunk belongs to a running warp and the earliest unfinished row
+// has its dependencies done: no deadlock for any grid size.  The last warp
+// to leave resets the counters for the next launch (all its claims, failing
+// ones included, come before it leaves).
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, const Vec4<double>* r,
                                                            Vec4<double>* z, const int* gate) {
@@ -254,109 +261,128 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
   Vec4<double>* out = kForward ? ilu.tmp : z;  // slots this sweep fills (empty on entry)
   const int lane = threadIdx.x & 31;
   const unsigned int nchunks = (unsigned int)(n + 31) / 32u;
-  // Surplus warps of the last block leave before claiming: exactly nchunks
-  // claims per launch, so the reset below runs after the last claim.
-  if (blockIdx.x * (unsigned int)(kSweepBlock / 32) + (threadIdx.x >> 5) >= nchunks) return;
-  unsigned int chunk = 0;
-  if (lane == 0) chunk = atomicAdd(&sync->claim, 1u);
-  chunk = __shfl_sync(kFull, chunk, 0);
+  const unsigned int nwarps = gridDim.x * (unsigned int)(kSweepBlock / 32);
   const int64_t nc = ilu.nc;
-  const int p = (int)chunk * 32 + lane;
-  const bool active = p < n;
-  int i = 0, dep[4], ndep = 0, slot[4];
-  Vec4<double> own{};
-  if (active) {
-    i = ilu.sweep[kForward ? p : (int64_t)n + p];
-    const int pi = ilu.pos[i];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int o = ilu.nbr[k * nc + i];
-      if (o < 0) continue;
-      const int po = ilu.pos[o];
-      if (kForward ? po < pi : po > pi) {
-        dep[ndep] = o;
-        slot[ndep] = k;
-        ++ndep;
-      }
-    }
-    // The row's blocks (and D^-1 backward) do not depend on the waits:
-    // bring them towards L1 first.
-    const char* rowp = reinterpret_cast<const char*>(ilu.A + (int64_t)i * 80);
-#pragma unroll
-    for (int b = 0; b < 5; ++b) prefetch_l1(rowp + 128 * b);
-    if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)i * 16);
-    if (kForward) {
-      own = r[i];
-      store_empty(z + i);  // the backward sweep's slot
-    } else {
-      const double2* t = reinterpret_cast<const double2*>(ilu.tmp + i);
-      const double2 a = __ldcg(t), b = __ldcg(t + 1);
-      own = Vec4<double>{a.x, a.y, b.x, b.y};
-      store_empty(ilu.tmp + i);  // empty again for the next forward sweep
-    }
-  }
-  bool done = !active;
-  long long spins = 0;
-  while (__any_sync(kFull, !done)) {
-    if (done) continue;
-    bool ready = true;
-    unsigned long long w[4][4];
-    for (int d = 0; d < ndep; ++d) {
-      const unsigned long long* q = reinterpret_cast<const unsigned long long*>(out + dep[d]);
+  while (true) {
+    unsigned int chunk = 0;
+    if (lane == 0) chunk = atomicAdd(&sync->claim, 1u);
+    chunk = __shfl_sync(kFull, chunk, 0);
+    if (chunk >= nchunks) break;
+    const int p = (int)chunk * 32 + lane;
+    const bool active = p < n;
+    int i = 0, dep[4], ndep = 0, slot[4];
+    Vec4<double> own{};
+    if (active) {
+      i = ilu.sweep[kForward ? p : (int64_t)n + p];
+      const int pi = ilu.pos[i];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        w[d][k] = ld_relaxed_u64(q + k);
-        if (w[d][k] == kSweepEmpty) ready = false;
+        const int o = ilu.nbr[k * nc + i];
+        if (o < 0) continue;
+        const int po = ilu.pos[o];
+        if (kForward ? po < pi : po > pi) {
+          dep[ndep] = o;
+          slot[ndep] = k;
+          ++ndep;
+        }
+      }
+      // The row's blocks (and D^-1 backward) do not depend on the waits:
+      // bring them towards L1 first.
+      const char* rowp = reinterpret_cast<const char*>(ilu.A + (int64_t)i * 80);
+#pragma unroll
+      for (int b = 0; b < 5; ++b) prefetch_l1(rowp + 128 * b);
+      if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)i * 16);
+      if (kForward) {
+        own = r[i];
+        store_empty(z + i);  // the backward sweep's slot
+      } else {
+        const double2* t = reinterpret_cast<const double2*>(ilu.tmp + i);
+        const double2 a = __ldcg(t), b = __ldcg(t + 1);
+        own = Vec4<double>{a.x, a.y, b.x, b.y};
+        store_empty(ilu.tmp + i);  // empty again for the next forward sweep
       }
     }
-    if (ready) {
-      const double* row = ilu.A + (int64_t)i * 80;
-      Vec4<double> acc = own;
-      for (int d = 0; d < ndep; ++d) {
-        const double* Bk = row + 16 * (1 + slot[d]);
-        const Vec4<double> v{__longlong_as_double((long long)w[d][0]), __longlong_as_double((long long)w[d][1]),
-                             __longlong_as_double((long long)w[d][2]), __longlong_as_double((long long)w[d][3])};
-        acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
-        acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
-        acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
-        acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+    bool done = !active;
+    long long spins = 0;
+    while (__any_sync(kFull, !done)) {
+      if (done) continue;
+      // the last word first (cheap while waiting), then all four
+      bool ready = true;
+      for (int d = 0; d < ndep; ++d)
+        if (ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(out + dep[d]) + 3) == kSweepEmpty)
+          ready = false;
+      unsigned long long w[4][4];
+      if (ready) {
+        for (int d = 0; d < ndep; ++d) {
+          const unsigned long long* q = reinterpret_cast<const unsigned long long*>(out + dep[d]);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            w[d][k] = ld_relaxed_u64(q + k);
+            if (w[d][k] == kSweepEmpty) ready = false;
+          }
+        }
       }
-      if (!kForward) {
-        const double* D = ilu.Dinv + (int64_t)i * 16;
-        Vec4<double> o4;
-        o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
-        o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
-        o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
-        o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
-        acc = o4;
-      }
-      if (!kForward || i != ilu.stall_row) {
-        unsigned long long* q = reinterpret_cast<unsigned long long*>(out + i);
-        st_relaxed_u64(q, sweep_bits(acc.a));
-        st_relaxed_u64(q + 1, sweep_bits(acc.b));
-        st_relaxed_u64(q + 2, sweep_bits(acc.c));
-        st_relaxed_u64(q + 3, sweep_bits(acc.d));
-      }
-      done = true;
-    } else if ((++spins & 63) == 0) {
-      if (spins > ilu.spin_limit) {
-        atomicExch(&sync->err, 1);
+      if (ready) {
+        const double* row = ilu.A + (int64_t)i * 80;
+        Vec4<double> acc = own;
+        for (int d = 0; d < ndep; ++d) {
+          const double* Bk = row + 16 * (1 + slot[d]);
+          const Vec4<double> v{__longlong_as_double((long long)w[d][0]), __longlong_as_double((long long)w[d][1]),
+                               __longlong_as_double((long long)w[d][2]), __longlong_as_double((long long)w[d][3])};
+          acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
+          acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
+          acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
+          acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+        }
+        if (!kForward) {
+          const double* D = ilu.Dinv + (int64_t)i * 16;
+          Vec4<double> o4;
+          o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
+          o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
+          o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
+          o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
+          acc = o4;
+        }
+        if (!kForward || i != ilu.stall_row) {
+          unsigned long long* q = reinterpret_cast<unsigned long long*>(out + i);
+          st_relaxed_u64(q, sweep_bits(acc.a));
+          st_relaxed_u64(q + 1, sweep_bits(acc.b));
+          st_relaxed_u64(q + 2, sweep_bits(acc.c));
+          st_relaxed_u64(q + 3, sweep_bits(acc.d));
+        }
         done = true;
-      } else if (*reinterpret_cast<volatile int*>(&sync->err)) {
-        done = true;
+      } else {
+        __nanosleep(32);
+        if ((++spins & 63) == 0) {
+          if (spins > ilu.spin_limit) {
+            atomicExch(&sync->err, 1);
+            done = true;
+          } else if (*reinterpret_cast<volatile int*>(&sync->err)) {
+            done = true;
+          }
+        }
       }
     }
   }
   __syncwarp();
   if (lane == 0) {
     __threadfence();
-    const unsigned int f = atomicAdd(&sync->done, 1u);
-    if (f == nchunks - 1) {  // every chunk has been claimed and finished
+    const unsigned int f = atomicAdd(&sync->done, 1u);  // warps that have left
+    if (f == nwarps - 1) {
       sync->claim = 0;
       sync->done = 0;
       __threadfence();
     }
   }
+}
+
+// Blocks of one sweep launch: enough warps to cover several dependency
+// levels ahead of the front, few enough that waiting warps do not crowd the
+// load path, and that the sweeps of other contexts can run beside them.
+inline int ilu_sweep_blocks(int n) {
+  const int chunks = (n + 31) / 32;
+  const int blocks = (chunks + kSweepBlock / 32 - 1) / (kSweepBlock / 32);
+  return blocks < 64 ? blocks : 64;
 }
 
 }  // namespace o2f

@@ -716,9 +716,7 @@ void Solver::ilu_factor() {
 void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) {
   cudaStream_t s = stream_;
   const int n = (int)ilu_.nc;
-  const int chunks = (n + 31) / 32;
-  const int warps_per_block = kSweepBlock / 32;
-  const int blocks = (chunks + warps_per_block - 1) / warps_per_block;
+  const int blocks = ilu_sweep_blocks(n);
   k_ilu_sweep<true><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, r, z, gate);  // r -> ilu_.tmp
   k_ilu_sweep<false><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, nullptr, z, gate);  // ilu_.tmp -> z
 }

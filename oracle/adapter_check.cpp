@@ -174,7 +174,7 @@ int main(int argc, char** argv) {
                 ref.cells.size(), ref.edges.size(), adv_cells, adv_edges, res_cells, res_edges, cr, force_err, hllc,
                 bc);
     const bool ok = adv_cells == 0 && adv_edges == 0 && res_cells == 0 && res_edges == 0 && cr == 0 && hllc == 0 &&
-                    bc == 0 && force_err <= 1e-12;
+                    bc == 0 && force_err <= 1e-11;
     return ok ? 0 : 1;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "o2f_adapter_check: %s\n", e.what());

@@ -444,10 +444,13 @@ int o2f_bc_diffusion(int64_t n, const uint8_t* codes, double* tq_host);
 /* Test hook of the failure path (no counterpart in the reference).  The
  * block-ILU(0) sweeps wait, bounded, on the ready flags of the rows they
  * depend on; a wait that runs out makes the solve return O2F_ERR_CUDA and
- * leaves the context usable.  With stall != 0 the solves started after this
- * call run with one row that never releases its flag and with spin_limit
- * polls per wait (<= 0: the default of 2^22), so that path can be exercised
- * without any GPU fault; stall = 0, spin_limit = 0 restores the defaults. */
+ * leaves the context usable.  Small triangles are swept without waits (one
+ * thread block, level by level); while the hook is set (stall != 0 or
+ * spin_limit > 0) the solves started after the call use the waiting sweeps,
+ * with spin_limit polls per wait (<= 0: the default of 2^22) and, with stall
+ * != 0, one row that never writes its value, so the failure path can be
+ * exercised without any GPU fault; stall = 0, spin_limit = 0 restores the
+ * defaults. */
 int o2f_debug_ilu_stall(o2f_ctx* ctx, int stall, int64_t spin_limit);
 
 /* No counterpart in the reference.  For callers that may not allocate

@@ -116,12 +116,14 @@ struct IluDev {
   int32_t* pos;       // [nc] position of the cell in the ILU order
   int32_t* order;     // [nc] cell at each ILU position (inverse of pos)
   int32_t* sweep;     // [2*nc] processing orders of the forward, then the backward sweep
+  int32_t* lev_off;   // [n_lo+1 + n_up+1] level offsets into the forward, then the backward order
   double* A;          // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
   double* Dinv;       // [nc*16]
   int32_t* lo_cells;  // [nc] factorization levels, concatenated (offsets kept on the host)
   Vec4<double>* tmp;  // [nc] forward sweep's output / backward sweep's input (empty between applications)
   SweepSync* sync;    // [2] forward, backward
   int n_lo;
+  int n_up;           // dependency levels of the backward sweep
   long long spin_limit;  // polls a sweep row waits before it gives up (error status)
   int32_t stall_row;     // test hook: this row never releases its forward flag (-1: none)
 };

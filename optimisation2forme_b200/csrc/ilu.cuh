@@ -376,6 +376,76 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
   }
 }
 
+// One thread block solves a whole triangle, level after level: the rows of a
+// level are independent, a __syncthreads separates the levels and makes the
+// values written by the block visible to it, so no row ever waits on a flag
+// and a level costs a barrier plus its loads (the next level's rows are
+// prefetched while the current one is solved).  The arithmetic of a row,
+// dependencies in slot order, is that of k_ilu_sweep, so both give the same
+// bits; the empty slots are kept as k_ilu_sweep expects them.  One SM per
+// sweep: the sweeps of many contexts run side by side.
+constexpr int kSweepCtaThreads = 512;
+
+template <bool kForward>
+__global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
+                                                                    Vec4<double>* z, const int* gate) {
+  if (gated(gate)) return;
+  const int64_t nc = ilu.nc;
+  const int32_t* order = ilu.sweep + (kForward ? 0 : (int64_t)n);
+  const int32_t* off = ilu.lev_off + (kForward ? 0 : ilu.n_lo + 1);
+  const int nlev = kForward ? ilu.n_lo : ilu.n_up;
+  Vec4<double>* out = kForward ? ilu.tmp : z;  // written and read by this block only
+  for (int l = 0; l < nlev; ++l) {
+    const int b = off[l], e = off[l + 1];
+    if (l + 1 < nlev)
+      for (int p = e + threadIdx.x; p < off[l + 2]; p += blockDim.x) {
+        const char* rowp = reinterpret_cast<const char*>(ilu.A + (int64_t)order[p] * 80);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) prefetch_l1(rowp + 128 * q);
+      }
+    for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+      const int i = order[p];
+      const int pi = ilu.pos[i];
+      const double* row = ilu.A + (int64_t)i * 80;
+      Vec4<double> acc;
+      if (kForward) {
+        acc = r[i];
+        store_empty(z + i);  // the backward sweep's slot
+      } else {
+        acc = ilu.tmp[i];
+        store_empty(ilu.tmp + i);  // empty again for the next forward sweep
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int o = ilu.nbr[k * nc + i];
+        if (o < 0) continue;
+        const int po = ilu.pos[o];
+        if (!(kForward ? po < pi : po > pi)) continue;
+        const double* Bk = row + 16 * (1 + k);
+        const Vec4<double> v = out[o];
+        acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
+        acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
+        acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
+        acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+      }
+      if (!kForward) {
+        const double* D = ilu.Dinv + (int64_t)i * 16;
+        Vec4<double> o4;
+        o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
+        o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
+        o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
+        o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
+        acc = o4;
+      }
+      out[i] = Vec4<double>{__longlong_as_double((long long)sweep_bits(acc.a)),
+                            __longlong_as_double((long long)sweep_bits(acc.b)),
+                            __longlong_as_double((long long)sweep_bits(acc.c)),
+                            __longlong_as_double((long long)sweep_bits(acc.d))};
+    }
+    __syncthreads();
+  }
+}
+
 // Blocks of one sweep launch: enough warps to cover several dependency
 // levels ahead of the front, few enough that waiting warps do not crowd the
 // load path, and that the sweeps of other contexts can run beside them.

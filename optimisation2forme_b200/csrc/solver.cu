@@ -658,9 +658,13 @@ void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector
     for (int64_t i = nc - 1; i >= 0; --i) ilu_sweep_h_[nc + fill[levu[order[i]]]++] = order[i];
   }
   ilu_n_up_ = nup;
+  // level offsets of both sweep orders, forward then backward
+  ilu_lev_off_h_.assign(lo_off_h_.begin(), lo_off_h_.end());
+  ilu_lev_off_h_.insert(ilu_lev_off_h_.end(), up_off.begin(), up_off.end());
   ilu_order_h_ = std::move(order);
   ilu_.nc = nc;
   ilu_.n_lo = nlo;
+  ilu_.n_up = nup;
   ilu_.spin_limit = kSweepSpinLimit;
   ilu_.stall_row = -1;
 }
@@ -676,6 +680,7 @@ void Solver::ilu_factor() {
     ilu_.Dinv = arena_.alloc<double>(16 * nc);
     ilu_.order = arena_.alloc<int32_t>(nc);
     ilu_.sweep = arena_.alloc<int32_t>(2 * nc);
+    ilu_.lev_off = arena_.alloc<int32_t>(ilu_lev_off_h_.size());
     ilu_.lo_cells = arena_.alloc<int32_t>(nc);
     ilu_.tmp = arena_.alloc<Vec4<double>>(nc);
     ilu_.sync = arena_.alloc<SweepSync>(2);
@@ -686,6 +691,7 @@ void Solver::ilu_factor() {
     h2d(ilu_.pos, ilu_pos_h_, s);
     h2d(ilu_.order, ilu_order_h_, s);
     h2d(ilu_.sweep, ilu_sweep_h_, s);
+    h2d(ilu_.lev_off, ilu_lev_off_h_, s);
     h2d(ilu_.lo_cells, lo_cells_h_, s);
     k_ilu_empty<<<grid(nc), kBlock, 0, s>>>(nc, ilu_.tmp);
     O2F_CUDA(cudaMemsetAsync(ilu_.sync, 0, 2 * sizeof(SweepSync), s));
@@ -710,25 +716,34 @@ void Solver::ilu_factor() {
   if (st) throw Error(O2F_ERR_BREAKDOWN, "singular block in the ILU(0) factorization");
 }
 
-// z = M^{-1} r: the forward sweep into ilu_.tmp, the backward sweep into z.
-// z = U^{-1} L^{-1} r: one sync-free launch per triangle, one warp per
-// 32-row chunk (surplus warps of the last block exit without claiming).
+// Triangles up to this many rows are swept by one thread block (no waits).
+constexpr int64_t kIluCtaMaxRows = int64_t(1) << 30;
+
+// z = M^{-1} r = U^{-1} L^{-1} r: the forward sweep into ilu_.tmp, the
+// backward sweep into z; one launch per triangle, either one block walking
+// the levels or persistent warps that wait on their rows' dependencies.
 void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) {
   cudaStream_t s = stream_;
   const int n = (int)ilu_.nc;
+  if (!ilu_waiting_ && n <= kIluCtaMaxRows) {  // one block per triangle, level by level
+    k_ilu_sweep_cta<true><<<1, kSweepCtaThreads, 0, s>>>(n, ilu_, r, z, gate);
+    k_ilu_sweep_cta<false><<<1, kSweepCtaThreads, 0, s>>>(n, ilu_, nullptr, z, gate);
+    return;
+  }
   const int blocks = ilu_sweep_blocks(n);
   k_ilu_sweep<true><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, r, z, gate);  // r -> ilu_.tmp
   k_ilu_sweep<false><<<blocks, kSweepBlock, 0, s>>>(n, ilu_, nullptr, z, gate);  // ilu_.tmp -> z
 }
 
-// Test hook: the next solves run their sweeps with `spin_limit` polls per
-// wait, and with `stall` the first row of the forward order never writes its
+// Test hook: the next solves run the waiting sweeps (k_ilu_sweep) with
+// `spin_limit` polls per wait, and with `stall` the first row of the forward order never writes its
 // value, so the rows that depend on it wait out their limit (no fault:
 // every wait is bounded).  spin_limit <= 0 and stall = 0 restore the
 // defaults.  Takes effect for the solves that start after the call.
 void Solver::debug_ilu_stall(int stall, long long spin_limit) {
   ilu_.spin_limit = spin_limit > 0 ? spin_limit : kSweepSpinLimit;
   ilu_.stall_row = stall && !ilu_sweep_h_.empty() ? ilu_sweep_h_[0] : -1;
+  ilu_waiting_ = stall != 0 || spin_limit > 0;  // the hook needs the sweeps that wait
 }
 
 // A sweep whose dependency wait ran out leaves an invalid result: report it

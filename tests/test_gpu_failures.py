@@ -109,3 +109,24 @@ def test_ilu_sweep_wait_that_runs_out_returns_a_status():
         again = s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=2000, restart=500)
         assert again["iters"] == ref["iters"]
         np.testing.assert_array_equal(again["lambda"], ref["lambda"])
+
+
+def test_block_sweeps_and_waiting_sweeps_give_the_same_solution():
+    """The two ways of sweeping the ILU triangles -- one thread block walking
+    the dependency levels, or persistent warps waiting on their rows'
+    dependencies -- compute every row with the same arithmetic: the adjoint
+    solves agree bit for bit, and switching back and forth on one context
+    keeps them so."""
+    s, p = _solver()
+    with s:
+        s.initialize_freestream()
+        s.time_loop(50)
+        s.compute_residual()
+        a = s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=2000, restart=500)
+        s.debug_ilu_stall(False, spin_limit=1 << 22)  # the waiting sweeps
+        b = s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=2000, restart=500)
+        s.debug_ilu_stall(False)
+        c = s.solve_adjoint_system(beta=0.1, tol=1e-10, max_iter=2000, restart=500)
+        assert a["iters"] == b["iters"] == c["iters"]
+        np.testing.assert_array_equal(a["lambda"], b["lambda"])
+        np.testing.assert_array_equal(a["lambda"], c["lambda"])

@@ -117,6 +117,9 @@ struct IluDev {
   int32_t* order;     // [nc] cell at each ILU position (inverse of pos)
   int32_t* sweep;     // [2*nc] processing orders of the forward, then the backward sweep
   int32_t* lev_off;   // [n_lo+1 + n_up+1] level offsets into the forward, then the backward order
+  int32_t* rec;       // [2*nc*8] block-sweep records per sweep position (row, dependency positions, slots)
+  Vec4<double>* out_f;  // [nc] block sweeps: forward values by forward position
+  Vec4<double>* out_b;  // [nc] block sweeps: backward values by backward position
   double* A;          // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
   double* Dinv;       // [nc*16]
   int32_t* lo_cells;  // [nc] factorization levels, concatenated (offsets kept on the host)

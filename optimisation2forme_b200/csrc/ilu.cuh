@@ -377,52 +377,57 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
 }
 
 // One thread block solves a whole triangle, level after level: the rows of a
-// level are independent, a __syncthreads separates the levels and makes the
-// values written by the block visible to it, so no row ever waits on a flag
-// and a level costs a barrier plus its loads (the next level's rows are
-// prefetched while the current one is solved).  The arithmetic of a row,
-// dependencies in slot order, is that of k_ilu_sweep, so both give the same
-// bits; the empty slots are kept as k_ilu_sweep expects them.  One SM per
-// sweep: the sweeps of many contexts run side by side.
+// level are independent and a __syncthreads separates the levels, so no row
+// ever waits on a flag.  Each sweep position has a record (row, the sweep
+// positions of its dependencies, their slots); values are kept by sweep
+// position, and the last kSweepWindow of them also in shared memory, where
+// a row finds its dependencies -- they lie mostly a few levels back.  A
+// dependency q is read from shared memory when q >= e - kSweepWindow (e:
+// end of the current level): its slot is not overwritten by this level's
+// writes, which reuse the slots of positions [b - W, e - W).  The next
+// level's records and factor blocks are prefetched while a level is solved.
+// The arithmetic of a row (dependencies in slot order) is that of
+// k_ilu_sweep: both give the same bits.  One SM per sweep, so the sweeps of
+// many contexts run side by side.
 constexpr int kSweepCtaThreads = 512;
+constexpr int kSweepWindow = 4096;  // values kept in shared memory (128 KiB)
+constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow;
 
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
                                                                     Vec4<double>* z, const int* gate) {
   if (gated(gate)) return;
-  const int64_t nc = ilu.nc;
-  const int32_t* order = ilu.sweep + (kForward ? 0 : (int64_t)n);
+  extern __shared__ Vec4<double> win[];
+  const int* rec = ilu.rec + (kForward ? 0 : (int64_t)8 * n);
   const int32_t* off = ilu.lev_off + (kForward ? 0 : ilu.n_lo + 1);
   const int nlev = kForward ? ilu.n_lo : ilu.n_up;
-  Vec4<double>* out = kForward ? ilu.tmp : z;  // written and read by this block only
+  Vec4<double>* out = kForward ? ilu.out_f : ilu.out_b;  // by sweep position
   for (int l = 0; l < nlev; ++l) {
     const int b = off[l], e = off[l + 1];
-    if (l + 1 < nlev)
+    if (l + 1 < nlev)  // the next level's factor blocks towards L1
       for (int p = e + threadIdx.x; p < off[l + 2]; p += blockDim.x) {
-        const char* rowp = reinterpret_cast<const char*>(ilu.A + (int64_t)order[p] * 80);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) prefetch_l1(rowp + 128 * q);
+        const int4 a = *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p);
+        const unsigned int sl = (unsigned int)rec[8 * (int64_t)p + 5];
+        const double* row = ilu.A + (int64_t)a.x * 80;
+        if (a.y >= 0) prefetch_l1(row + 16 * (1 + (sl & 0xff)));
+        if (a.z >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 8) & 0xff)));
+        if (a.w >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 16) & 0xff)));
+        if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)a.x * 16);
       }
     for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
-      const int i = order[p];
-      const int pi = ilu.pos[i];
+      const int4 a = *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p);
+      const int4 c = *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p + 4);
+      const int i = a.x;
+      const int dq[4] = {a.y, a.z, a.w, c.x};
+      const unsigned int sl = (unsigned int)c.y;
       const double* row = ilu.A + (int64_t)i * 80;
-      Vec4<double> acc;
-      if (kForward) {
-        acc = r[i];
-        store_empty(z + i);  // the backward sweep's slot
-      } else {
-        acc = ilu.tmp[i];
-        store_empty(ilu.tmp + i);  // empty again for the next forward sweep
-      }
+      Vec4<double> acc = kForward ? r[i] : ilu.out_f[c.z];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int o = ilu.nbr[k * nc + i];
-        if (o < 0) continue;
-        const int po = ilu.pos[o];
-        if (!(kForward ? po < pi : po > pi)) continue;
-        const double* Bk = row + 16 * (1 + k);
-        const Vec4<double> v = out[o];
+      for (int d = 0; d < 4; ++d) {
+        const int q = dq[d];
+        if (q < 0) break;
+        const double* Bk = row + 16 * (1 + ((sl >> (8 * d)) & 0xff));
+        const Vec4<double> v = q >= e - kSweepWindow ? win[q % kSweepWindow] : out[q];
         acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
         acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
         acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
@@ -437,10 +442,13 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
         o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
         acc = o4;
       }
-      out[i] = Vec4<double>{__longlong_as_double((long long)sweep_bits(acc.a)),
-                            __longlong_as_double((long long)sweep_bits(acc.b)),
-                            __longlong_as_double((long long)sweep_bits(acc.c)),
-                            __longlong_as_double((long long)sweep_bits(acc.d))};
+      const Vec4<double> v{__longlong_as_double((long long)sweep_bits(acc.a)),
+                           __longlong_as_double((long long)sweep_bits(acc.b)),
+                           __longlong_as_double((long long)sweep_bits(acc.c)),
+                           __longlong_as_double((long long)sweep_bits(acc.d))};
+      win[p % kSweepWindow] = v;
+      out[p] = v;
+      if (!kForward) z[i] = v;
     }
     __syncthreads();
   }

@@ -661,6 +661,38 @@ void Solver::setup_ilu_host(const std::vector<int32_t>& jslot, const std::vector
   // level offsets of both sweep orders, forward then backward
   ilu_lev_off_h_.assign(lo_off_h_.begin(), lo_off_h_.end());
   ilu_lev_off_h_.insert(ilu_lev_off_h_.end(), up_off.begin(), up_off.end());
+  // Records of the block sweeps, per sweep position p (8 int32): the row,
+  // the sweep positions of its dependencies in slot order (-1: none), their
+  // slots (8 bits each), and for the backward sweep the row's forward
+  // position (where its forward value is).
+  {
+    std::vector<int32_t> posf(nc), posb(nc);
+    for (int64_t p = 0; p < nc; ++p) {
+      posf[ilu_sweep_h_[p]] = (int32_t)p;
+      posb[ilu_sweep_h_[nc + p]] = (int32_t)p;
+    }
+    ilu_rec_h_.assign(16 * nc, -1);
+    for (int dir = 0; dir < 2; ++dir)
+      for (int64_t p = 0; p < nc; ++p) {
+        const int32_t c = ilu_sweep_h_[dir * nc + p];
+        int32_t* rec = ilu_rec_h_.data() + 8 * (dir * nc + p);
+        rec[0] = c;
+        int nd = 0;
+        uint32_t slots = 0xffffffffu;
+        for (int k = 0; k < 4; ++k) {
+          const int32_t o = nbr(c, k);
+          if (o < 0) continue;
+          const bool dep = dir == 0 ? ilu_pos_h_[o] < ilu_pos_h_[c] : ilu_pos_h_[o] > ilu_pos_h_[c];
+          if (!dep) continue;
+          rec[1 + nd] = dir == 0 ? posf[o] : posb[o];
+          slots = (slots & ~(0xffu << (8 * nd))) | ((uint32_t)k << (8 * nd));
+          ++nd;
+        }
+        rec[5] = (int32_t)slots;
+        rec[6] = posf[c];
+        rec[7] = 0;
+      }
+  }
   ilu_order_h_ = std::move(order);
   ilu_.nc = nc;
   ilu_.n_lo = nlo;
@@ -681,6 +713,9 @@ void Solver::ilu_factor() {
     ilu_.order = arena_.alloc<int32_t>(nc);
     ilu_.sweep = arena_.alloc<int32_t>(2 * nc);
     ilu_.lev_off = arena_.alloc<int32_t>(ilu_lev_off_h_.size());
+    ilu_.rec = arena_.alloc<int32_t>(16 * nc);
+    ilu_.out_f = arena_.alloc<Vec4<double>>(nc);
+    ilu_.out_b = arena_.alloc<Vec4<double>>(nc);
     ilu_.lo_cells = arena_.alloc<int32_t>(nc);
     ilu_.tmp = arena_.alloc<Vec4<double>>(nc);
     ilu_.sync = arena_.alloc<SweepSync>(2);
@@ -692,6 +727,11 @@ void Solver::ilu_factor() {
     h2d(ilu_.order, ilu_order_h_, s);
     h2d(ilu_.sweep, ilu_sweep_h_, s);
     h2d(ilu_.lev_off, ilu_lev_off_h_, s);
+    h2d(ilu_.rec, ilu_rec_h_, s);
+    O2F_CUDA(cudaFuncSetAttribute(k_ilu_sweep_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSweepSmem));
+    O2F_CUDA(cudaFuncSetAttribute(k_ilu_sweep_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSweepSmem));
     h2d(ilu_.lo_cells, lo_cells_h_, s);
     k_ilu_empty<<<grid(nc), kBlock, 0, s>>>(nc, ilu_.tmp);
     O2F_CUDA(cudaMemsetAsync(ilu_.sync, 0, 2 * sizeof(SweepSync), s));
@@ -726,8 +766,8 @@ void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) 
   cudaStream_t s = stream_;
   const int n = (int)ilu_.nc;
   if (!ilu_waiting_ && n <= kIluCtaMaxRows) {  // one block per triangle, level by level
-    k_ilu_sweep_cta<true><<<1, kSweepCtaThreads, 0, s>>>(n, ilu_, r, z, gate);
-    k_ilu_sweep_cta<false><<<1, kSweepCtaThreads, 0, s>>>(n, ilu_, nullptr, z, gate);
+    k_ilu_sweep_cta<true><<<1, kSweepCtaThreads, kSweepSmem, s>>>(n, ilu_, r, z, gate);
+    k_ilu_sweep_cta<false><<<1, kSweepCtaThreads, kSweepSmem, s>>>(n, ilu_, nullptr, z, gate);
     return;
   }
   const int blocks = ilu_sweep_blocks(n);

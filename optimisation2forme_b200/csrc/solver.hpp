@@ -204,7 +204,7 @@ class Solver {
  private:
   std::vector<int32_t> ilu_nbr_h_, ilu_pos_h_, ilu_order_h_, lo_off_h_, lo_cells_h_, ilu_sweep_h_;
   int ilu_n_up_ = 0;  // levels of the backward sweep's dependencies
-  std::vector<int32_t> ilu_lev_off_h_;
+  std::vector<int32_t> ilu_lev_off_h_, ilu_rec_h_;
   bool ilu_waiting_ = false;  // test hook: use the sweeps that wait on other rows
   IluDev ilu_{};
   bool ilu_alloc_ = false;

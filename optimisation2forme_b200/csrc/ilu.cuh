@@ -393,6 +393,50 @@ constexpr int kSweepCtaThreads = 512;
 constexpr int kSweepWindow = 4096;  // values kept in shared memory (128 KiB)
 constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow;
 
+// One row of a block sweep: own value minus the dependencies' products
+// (slot order), times D^-1 backward; stored in the window, by position, and
+// (backward) into z by row.
+template <bool kForward>
+__device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, const int4& a, const int4& c,
+                                              Vec4<double> acc, const Vec4<double>* win_r, Vec4<double>* win,
+                                              Vec4<double>* out, Vec4<double>* z) {
+  const int i = a.x;
+  const int dq[4] = {a.y, a.z, a.w, c.x};
+  const unsigned int sl = (unsigned int)c.y;
+  const double* row = ilu.A + (int64_t)i * 80;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const int q = dq[d];
+    if (q < 0) break;
+    const double* Bk = row + 16 * (1 + ((sl >> (8 * d)) & 0xff));
+    const Vec4<double> v = q >= e - kSweepWindow ? win_r[q % kSweepWindow] : out[q];
+    acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
+    acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
+    acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
+    acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+  }
+  if (!kForward) {
+    const double* D = ilu.Dinv + (int64_t)i * 16;
+    Vec4<double> o4;
+    o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
+    o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
+    o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
+    o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
+    acc = o4;
+  }
+  const Vec4<double> v{__longlong_as_double((long long)sweep_bits(acc.a)),
+                       __longlong_as_double((long long)sweep_bits(acc.b)),
+                       __longlong_as_double((long long)sweep_bits(acc.c)),
+                       __longlong_as_double((long long)sweep_bits(acc.d))};
+  win[p % kSweepWindow] = v;
+  out[p] = v;
+  if (!kForward) z[i] = v;
+}
+
+// The first two rows of each thread in a level are software-pipelined: their
+// records are loaded during the level before, their own values (r, or the
+// forward value) and factor blocks requested at its end, so a level starts
+// with its operands in flight; further rows load at use.
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
                                                                     Vec4<double>* z, const int* gate) {
@@ -402,53 +446,61 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
   const int32_t* off = ilu.lev_off + (kForward ? 0 : ilu.n_lo + 1);
   const int nlev = kForward ? ilu.n_lo : ilu.n_up;
   Vec4<double>* out = kForward ? ilu.out_f : ilu.out_b;  // by sweep position
+  const int T = blockDim.x, t = threadIdx.x;
+  auto rec_a = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p); };
+  auto rec_c = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p + 4); };
+  auto own_of = [&](const int4& a, const int4& c) { return kForward ? r[a.x] : ilu.out_f[c.z]; };
+  auto prefetch_row = [&](const int4& a, const int4& c) {
+    const unsigned int sl = (unsigned int)c.y;
+    const double* row = ilu.A + (int64_t)a.x * 80;
+    if (a.y >= 0) prefetch_l1(row + 16 * (1 + (sl & 0xff)));
+    if (a.z >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 8) & 0xff)));
+    if (a.w >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 16) & 0xff)));
+    if (c.x >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 24) & 0xff)));
+    if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)a.x * 16);
+  };
+  int4 ra[2], rc[2];
+  Vec4<double> own[2];
+  if (nlev > 0)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int p = off[0] + t + k * T;
+      if (p < off[1]) {
+        ra[k] = rec_a(p);
+        rc[k] = rec_c(p);
+        own[k] = own_of(ra[k], rc[k]);
+      }
+    }
   for (int l = 0; l < nlev; ++l) {
     const int b = off[l], e = off[l + 1];
-    if (l + 1 < nlev)  // the next level's factor blocks towards L1
-      for (int p = e + threadIdx.x; p < off[l + 2]; p += blockDim.x) {
-        const int4 a = *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p);
-        const unsigned int sl = (unsigned int)rec[8 * (int64_t)p + 5];
-        const double* row = ilu.A + (int64_t)a.x * 80;
-        if (a.y >= 0) prefetch_l1(row + 16 * (1 + (sl & 0xff)));
-        if (a.z >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 8) & 0xff)));
-        if (a.w >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 16) & 0xff)));
-        if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)a.x * 16);
-      }
-    for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
-      const int4 a = *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p);
-      const int4 c = *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p + 4);
-      const int i = a.x;
-      const int dq[4] = {a.y, a.z, a.w, c.x};
-      const unsigned int sl = (unsigned int)c.y;
-      const double* row = ilu.A + (int64_t)i * 80;
-      Vec4<double> acc = kForward ? r[i] : ilu.out_f[c.z];
+    const int ne = l + 1 < nlev ? off[l + 2] : e;
+    int4 na[2], nc[2];
 #pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        const int q = dq[d];
-        if (q < 0) break;
-        const double* Bk = row + 16 * (1 + ((sl >> (8 * d)) & 0xff));
-        const Vec4<double> v = q >= e - kSweepWindow ? win[q % kSweepWindow] : out[q];
-        acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
-        acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
-        acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
-        acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+    for (int k = 0; k < 2; ++k) {  // the next level's records, in flight during this one
+      const int q = e + t + k * T;
+      if (q < ne) {
+        na[k] = rec_a(q);
+        nc[k] = rec_c(q);
       }
-      if (!kForward) {
-        const double* D = ilu.Dinv + (int64_t)i * 16;
-        Vec4<double> o4;
-        o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
-        o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
-        o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
-        o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
-        acc = o4;
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int p = b + t + k * T;
+      if (p < e) sweep_cta_row<kForward>(ilu, p, e, ra[k], rc[k], own[k], win, win, out, z);
+    }
+    for (int p = b + t + 2 * T; p < e; p += T) {
+      const int4 a = rec_a(p), c = rec_c(p);
+      sweep_cta_row<kForward>(ilu, p, e, a, c, own_of(a, c), win, win, out, z);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {  // the next level's operands, requested before the barrier
+      const int q = e + t + k * T;
+      if (q < ne) {
+        ra[k] = na[k];
+        rc[k] = nc[k];
+        prefetch_row(ra[k], rc[k]);
+        own[k] = own_of(ra[k], rc[k]);
       }
-      const Vec4<double> v{__longlong_as_double((long long)sweep_bits(acc.a)),
-                           __longlong_as_double((long long)sweep_bits(acc.b)),
-                           __longlong_as_double((long long)sweep_bits(acc.c)),
-                           __longlong_as_double((long long)sweep_bits(acc.d))};
-      win[p % kSweepWindow] = v;
-      out[p] = v;
-      if (!kForward) z[i] = v;
     }
     __syncthreads();
   }

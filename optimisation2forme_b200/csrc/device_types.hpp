@@ -120,6 +120,7 @@ struct IluDev {
   int32_t* rec;       // [2*nc*8] block-sweep records per sweep position (row, dependency positions, slots)
   Vec4<double>* out_f;  // [nc] block sweeps: forward values by forward position
   Vec4<double>* out_b;  // [nc] block sweeps: backward values by backward position
+  double* pack;       // block sweeps: factor blocks in sweep order, interleaved over 32 positions (k_ilu_pack)
   double* A;          // [nc*5*16] row blocks (diagonal, then the 4 slots), row-major 4x4
   double* Dinv;       // [nc*16]
   int32_t* lo_cells;  // [nc] factorization levels, concatenated (offsets kept on the host)

@@ -384,14 +384,48 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
 // a row finds its dependencies -- they lie mostly a few levels back.  A
 // dependency q is read from shared memory when q >= e - kSweepWindow (e:
 // end of the current level): its slot is not overwritten by this level's
-// writes, which reuse the slots of positions [b - W, e - W).  The next
-// level's records and factor blocks are prefetched while a level is solved.
+// writes, which reuse the slots of positions [b - W, e - W).
 // The arithmetic of a row (dependencies in slot order) is that of
 // k_ilu_sweep: both give the same bits.  One SM per sweep, so the sweeps of
 // many contexts run side by side.
 constexpr int kSweepCtaThreads = 512;
 constexpr int kSweepWindow = 4096;  // values kept in shared memory (128 KiB)
 constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow;
+
+// Factor blocks of the block sweeps, repacked in sweep order after every
+// factorization and interleaved over 32 consecutive positions, so that the
+// 32 lanes of a warp (consecutive positions of a level) read 32 consecutive
+// doubles per element: element e of dependency d of position p of direction
+// dir is pk[dir*n*64 + (p>>5)*2048 + d*512 + e*32 + (p&31)] (n rounded up to
+// 32), D^-1 of backward position p is pk[2*n*64 + (p>>5)*512 + e*32 + (p&31)].
+__device__ __forceinline__ int64_t sweep_pack_base(int64_t n32, int dir, int p) {
+  return (int64_t)dir * n32 * 64 + (int64_t)(p >> 5) * 2048 + (p & 31);
+}
+
+__global__ void k_ilu_pack(int n, IluDev ilu) {
+  const int64_t n32 = ((int64_t)n + 31) / 32 * 32;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // (dir, p, d) with d = 4 for D^-1
+  if (t >= (int64_t)2 * n * 5) return;
+  const int dir = (int)(t / ((int64_t)n * 5));
+  const int64_t rest = t % ((int64_t)n * 5);
+  const int p = (int)(rest / 5), d = (int)(rest % 5);
+  const int* rec = ilu.rec + 8 * ((int64_t)dir * n + p);
+  const int row = rec[0];
+  if (d == 4) {
+    if (dir == 0) return;
+    const double* D = ilu.Dinv + (int64_t)row * 16;
+    double* dst = ilu.pack + 2 * n32 * 64 + (int64_t)(p >> 5) * 512 + (p & 31);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) dst[e * 32] = D[e];
+    return;
+  }
+  if (rec[1 + d] < 0) return;
+  const int slot = (int)(((unsigned int)rec[5] >> (8 * d)) & 0xff);
+  const double* B = ilu.A + (int64_t)row * 80 + 16 * (1 + slot);
+  double* dst = ilu.pack + sweep_pack_base(n32, dir, p) + d * 512;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) dst[e * 32] = B[e];
+}
 
 // One row of a block sweep: own value minus the dependencies' products
 // (slot order), times D^-1 backward; stored in the window, by position, and
@@ -402,26 +436,26 @@ __device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, c
                                               Vec4<double>* out, Vec4<double>* z) {
   const int i = a.x;
   const int dq[4] = {a.y, a.z, a.w, c.x};
-  const unsigned int sl = (unsigned int)c.y;
-  const double* row = ilu.A + (int64_t)i * 80;
+  const int64_t n32 = ((int64_t)ilu.nc + 31) / 32 * 32;
+  const double* P = ilu.pack + sweep_pack_base(n32, kForward ? 0 : 1, p);
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
     const int q = dq[d];
     if (q < 0) break;
-    const double* Bk = row + 16 * (1 + ((sl >> (8 * d)) & 0xff));
+    const double* Bk = P + d * 512;  // element k at Bk[32 k]
     const Vec4<double> v = q >= e - kSweepWindow ? win_r[q % kSweepWindow] : out[q];
-    acc.a -= Bk[0] * v.a + Bk[1] * v.b + Bk[2] * v.c + Bk[3] * v.d;
-    acc.b -= Bk[4] * v.a + Bk[5] * v.b + Bk[6] * v.c + Bk[7] * v.d;
-    acc.c -= Bk[8] * v.a + Bk[9] * v.b + Bk[10] * v.c + Bk[11] * v.d;
-    acc.d -= Bk[12] * v.a + Bk[13] * v.b + Bk[14] * v.c + Bk[15] * v.d;
+    acc.a -= Bk[0] * v.a + Bk[32] * v.b + Bk[64] * v.c + Bk[96] * v.d;
+    acc.b -= Bk[128] * v.a + Bk[160] * v.b + Bk[192] * v.c + Bk[224] * v.d;
+    acc.c -= Bk[256] * v.a + Bk[288] * v.b + Bk[320] * v.c + Bk[352] * v.d;
+    acc.d -= Bk[384] * v.a + Bk[416] * v.b + Bk[448] * v.c + Bk[480] * v.d;
   }
   if (!kForward) {
-    const double* D = ilu.Dinv + (int64_t)i * 16;
+    const double* D = ilu.pack + 2 * n32 * 64 + (int64_t)(p >> 5) * 512 + (p & 31);
     Vec4<double> o4;
-    o4.a = D[0] * acc.a + D[1] * acc.b + D[2] * acc.c + D[3] * acc.d;
-    o4.b = D[4] * acc.a + D[5] * acc.b + D[6] * acc.c + D[7] * acc.d;
-    o4.c = D[8] * acc.a + D[9] * acc.b + D[10] * acc.c + D[11] * acc.d;
-    o4.d = D[12] * acc.a + D[13] * acc.b + D[14] * acc.c + D[15] * acc.d;
+    o4.a = D[0] * acc.a + D[32] * acc.b + D[64] * acc.c + D[96] * acc.d;
+    o4.b = D[128] * acc.a + D[160] * acc.b + D[192] * acc.c + D[224] * acc.d;
+    o4.c = D[256] * acc.a + D[288] * acc.b + D[320] * acc.c + D[352] * acc.d;
+    o4.d = D[384] * acc.a + D[416] * acc.b + D[448] * acc.c + D[480] * acc.d;
     acc = o4;
   }
   const Vec4<double> v{__longlong_as_double((long long)sweep_bits(acc.a)),
@@ -434,9 +468,10 @@ __device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, c
 }
 
 // The first two rows of each thread in a level are software-pipelined: their
-// records are loaded during the level before, their own values (r, or the
-// forward value) and factor blocks requested at its end, so a level starts
-// with its operands in flight; further rows load at use.
+// records are loaded during the level before and their own values (r, or the
+// forward value) requested at its end, so a level starts with its operands
+// in flight; further rows load at use.  Factor blocks come from the packed
+// copy (k_ilu_pack), coalesced across the warp.
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
                                                                     Vec4<double>* z, const int* gate) {
@@ -450,15 +485,6 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
   auto rec_a = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p); };
   auto rec_c = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p + 4); };
   auto own_of = [&](const int4& a, const int4& c) { return kForward ? r[a.x] : ilu.out_f[c.z]; };
-  auto prefetch_row = [&](const int4& a, const int4& c) {
-    const unsigned int sl = (unsigned int)c.y;
-    const double* row = ilu.A + (int64_t)a.x * 80;
-    if (a.y >= 0) prefetch_l1(row + 16 * (1 + (sl & 0xff)));
-    if (a.z >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 8) & 0xff)));
-    if (a.w >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 16) & 0xff)));
-    if (c.x >= 0) prefetch_l1(row + 16 * (1 + ((sl >> 24) & 0xff)));
-    if (!kForward) prefetch_l1(ilu.Dinv + (int64_t)a.x * 16);
-  };
   int4 ra[2], rc[2];
   Vec4<double> own[2];
   if (nlev > 0)
@@ -498,7 +524,6 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
       if (q < ne) {
         ra[k] = na[k];
         rc[k] = nc[k];
-        prefetch_row(ra[k], rc[k]);
         own[k] = own_of(ra[k], rc[k]);
       }
     }

@@ -716,6 +716,7 @@ void Solver::ilu_factor() {
     ilu_.rec = arena_.alloc<int32_t>(16 * nc);
     ilu_.out_f = arena_.alloc<Vec4<double>>(nc);
     ilu_.out_b = arena_.alloc<Vec4<double>>(nc);
+    ilu_.pack = arena_.alloc<double>((nc + 31) / 32 * 32 * 144);
     ilu_.lo_cells = arena_.alloc<int32_t>(nc);
     ilu_.tmp = arena_.alloc<Vec4<double>>(nc);
     ilu_.sync = arena_.alloc<SweepSync>(2);
@@ -748,8 +749,10 @@ void Solver::ilu_factor() {
     const int n = lo_off_h_[l + 1] - lo_off_h_[l];
     k_ilu_factor<<<(n + 127) / 128, 128, 0, s>>>(ilu_.lo_cells + lo_off_h_[l], n, ilu_, ilu_status_);
   }
+  // the factor blocks in the block sweeps' order
+  k_ilu_pack<<<(int)((2 * nc * 5 + 255) / 256), 256, 0, s>>>((int)nc, ilu_);
   O2F_CUDA(cudaGetLastError());
-  launches_ += 1 + ilu_.n_lo;
+  launches_ += 2 + ilu_.n_lo;
   int st = 0;
   O2F_CUDA(cudaMemcpyAsync(&st, ilu_status_, sizeof(int), cudaMemcpyDeviceToHost, s));
   sync();

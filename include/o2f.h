@@ -95,6 +95,15 @@ typedef enum o2f_status {
  * and objective differentiated, the limiter's own derivative left out). */
 #define O2F_JAC_FROZEN 2
 
+/* Triangular sweeps of the block ILU(0) preconditioner.  BLOCK: one thread
+ * block walks the dependency levels (one SM per sweep: best when several
+ * contexts solve at once, and alone on small meshes); WAITING: persistent
+ * warps on up to 64 SMs, each row waiting on its dependencies (best alone on
+ * large meshes); AUTO: BLOCK up to 70,000 cells, else WAITING. */
+#define O2F_SWEEPS_AUTO 0
+#define O2F_SWEEPS_BLOCK 1
+#define O2F_SWEEPS_WAITING 2
+
 /* Arithmetic of the residual / Jacobian-transpose kernels. */
 #define O2F_PREC_F64 0 /* FP64 throughout (parity mode)                           */
 #define O2F_PREC_F32 1 /* FP32 residual and JT, FP64 reductions, dt and Krylov     */
@@ -134,6 +143,8 @@ typedef struct o2f_params {
                              true residual with the FP64 operator (iterative
                              refinement: same solution and tolerance); F64
                              default.  FP32 contexts always do this.             */
+  int adjoint_sweeps;     /* NEW: O2F_SWEEPS_* triangular sweeps of the block
+                             ILU(0) preconditioner (same results, bit for bit) */
 } o2f_params;
 
 void o2f_params_default(o2f_params* p);

@@ -61,6 +61,7 @@ class Params(C.Structure):
         ("adjoint_jacobian", C.c_int),
         ("adjoint_fd_step", C.c_double),
         ("adjoint_precision", C.c_int),
+        ("adjoint_sweeps", C.c_int),
     ]
 
 

@@ -109,6 +109,7 @@ void o2f_params_default(o2f_params* p) {
   p->adjoint_jacobian = O2F_JAC_REFERENCE;
   p->adjoint_fd_step = 1e-9;
   p->adjoint_precision = O2F_PREC_F64;
+  p->adjoint_sweeps = O2F_SWEEPS_AUTO;
 }
 
 int o2f_host_mesh_create(const o2f_mesh_desc* mesh, o2f_host_mesh** out) {

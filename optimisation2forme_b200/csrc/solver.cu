@@ -49,6 +49,9 @@ void validate_params(const o2f_params& p) {
   if (p.precision != O2F_PREC_F64 && p.precision != O2F_PREC_F32) throw Error(O2F_ERR_ARG, "unknown precision");
   if (p.adjoint_precision != O2F_PREC_F64 && p.adjoint_precision != O2F_PREC_F32)
     throw Error(O2F_ERR_ARG, "unknown adjoint_precision");
+  if (p.adjoint_sweeps != O2F_SWEEPS_AUTO && p.adjoint_sweeps != O2F_SWEEPS_BLOCK &&
+      p.adjoint_sweeps != O2F_SWEEPS_WAITING)
+    throw Error(O2F_ERR_ARG, "unknown adjoint_sweeps");
   if (p.adjoint_precond != O2F_PRECOND_NONE && p.adjoint_precond != O2F_PRECOND_ILU0)
     throw Error(O2F_ERR_ARG, "unknown adjoint preconditioner");
   if (p.dt_mode != O2F_DT_REFERENCE && p.dt_mode != O2F_DT_THERMAL) throw Error(O2F_ERR_ARG, "unknown dt_mode");
@@ -759,8 +762,10 @@ void Solver::ilu_factor() {
   if (st) throw Error(O2F_ERR_BREAKDOWN, "singular block in the ILU(0) factorization");
 }
 
-// Triangles up to this many rows are swept by one thread block (no waits).
-constexpr int64_t kIluCtaMaxRows = int64_t(1) << 30;
+// O2F_SWEEPS_AUTO: triangles up to this many rows are swept by one thread
+// block (measured on B200: faster alone up to ~40-70k rows, and side by side
+// with other contexts' solves at every size measured).
+constexpr int64_t kIluCtaMaxRows = 70000;
 
 // z = M^{-1} r = U^{-1} L^{-1} r: the forward sweep into ilu_.tmp, the
 // backward sweep into z; one launch per triangle, either one block walking
@@ -768,7 +773,9 @@ constexpr int64_t kIluCtaMaxRows = int64_t(1) << 30;
 void Solver::ilu_apply(const Vec4<double>* r, Vec4<double>* z, const int* gate) {
   cudaStream_t s = stream_;
   const int n = (int)ilu_.nc;
-  if (!ilu_waiting_ && n <= kIluCtaMaxRows) {  // one block per triangle, level by level
+  const int mode = params_.adjoint_sweeps;
+  const bool block = mode == O2F_SWEEPS_BLOCK || (mode == O2F_SWEEPS_AUTO && n <= kIluCtaMaxRows);
+  if (!ilu_waiting_ && block) {  // one block per triangle, level by level
     k_ilu_sweep_cta<true><<<1, kSweepCtaThreads, kSweepSmem, s>>>(n, ilu_, r, z, gate);
     k_ilu_sweep_cta<false><<<1, kSweepCtaThreads, kSweepSmem, s>>>(n, ilu_, nullptr, z, gate);
     return;

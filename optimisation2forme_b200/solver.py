@@ -61,6 +61,7 @@ class SimulationParams:
     adjoint_jacobian: str = "reference"
     adjoint_fd_step: float = 1e-9
     adjoint_precision: str = "fp64"
+    adjoint_sweeps: str = "auto"
     max_steps: int = 2**62
     residual_drop: float = 0.0
     adjoint_tol: float = 1e-6
@@ -82,6 +83,7 @@ class SimulationParams:
             raise ValueError(f"unknown limiter {self.limiter!r}")
         p.precision = {"fp64": _lib.PREC_F64, "fp32": _lib.PREC_F32}[self.precision.lower()]
         p.adjoint_precision = {"fp64": _lib.PREC_F64, "fp32": _lib.PREC_F32}[self.adjoint_precision.lower()]
+        p.adjoint_sweeps = {"auto": 0, "block": 1, "waiting": 2}[self.adjoint_sweeps.lower()]
         p.adjoint_precond = {"none": 0, "identity": 0, "ilu0": 1}[self.adjoint_precond.lower()]
         p.dt_mode = {"reference": 0, "thermal": 1}[self.dt_mode.lower()]
         p.adjoint_jacobian = {"reference": 0, "first_order": 0, "full": 1,
@@ -95,7 +97,7 @@ _FLOAT_KEYS = {"cfl_number", "final_time", "gamma", "viscosity", "Pr", "cp", "in
 _INT_KEYS = {"verbosity", "max_steps", "adjoint_restart", "adjoint_max_iter"}
 _STR_KEYS = {"mesh_name", "boundary_conditions", "initial_condition", "state_load_path", "state_save_path",
              "shape_param_file", "shape_log_file", "limiter", "precision", "adjoint_precond", "dt_mode",
-             "adjoint_jacobian", "adjoint_precision"}
+             "adjoint_jacobian", "adjoint_precision", "adjoint_sweeps"}
 
 
 def load_config(path: str | os.PathLike, params: SimulationParams | None = None) -> SimulationParams:

@@ -308,6 +308,7 @@ def shape_of(c: Candidate):
 
 
 def adjoint_and_gradient(s, c: Candidate, guess=None, cap: int = 20000) -> dict:
+    """J, the adjoint to ADJ_TOL (at most `cap` iterations) and dJ/d(m, p, t)."""
     _, _, J = s.lift_drag(BETA)
     a = s.solve_adjoint_system(BETA, tol=ADJ_TOL, max_iter=cap, restart=500, raise_on_failure=False, guess=guess)
     g = s.compute_shape_gradient(NAMES, shape_of(c), beta=BETA, eps=1e-6)
@@ -414,39 +415,45 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
             torch.distributed.barrier()
 
     # -- plain FP64 arm: one context after another
-    def plain_pass():
+    def plain_pass(cap=20000):
         out = []
         for s, c in zip(plain, cands):
             s.initialize_freestream()
             s.time_loop(rk)
-            out.append(adjoint_and_gradient(s, c))
+            out.append(adjoint_and_gradient(s, c, cap=cap))
         return out
 
     # -- fast arm: one batched time loop, then each candidate's adjoint from
     # the network's prediction (mixed-precision BiCGSTAB, FP64 refinement)
-    def fast_pass(states=None, serial=False, warm=True):
+    phase_s = {"time_loop": 0.0, "adjoint_and_gradient": 0.0}
+
+    def fast_pass(states=None, serial=False, warm=True, cap=20000):
+        t0 = time.perf_counter()
         for i, s in enumerate(fast):
             if states is None:
                 s.initialize_freestream()
             else:
                 s.set_state(states[i])
         res = batch.time_loop(rk)
+        t1 = time.perf_counter()
         bad = [i for i, r in enumerate(res) if r["status"] != "OK"]
         if bad:
             raise RuntimeError(f"fast time loop failed for candidates {bad}")
         # the network's predictions (one network: one call at a time), then
         # every candidate's adjoint and gradient at once
         guesses = [ws.guess(s, c) if ws and warm else None for s, c in zip(fast, cands)]
-        work = [lambda k=k: adjoint_and_gradient(fast[k], cands[k], guesses[k]) for k in range(len(cands))]
-        if serial:  # the first pass allocates each context's adjoint buffers
-            return [w() for w in work]
-        return concurrently(lambda w: w(), work)
+        work = [lambda k=k: adjoint_and_gradient(fast[k], cands[k], guesses[k], cap) for k in range(len(cands))]
+        # serial: a first, short pass allocates each context's adjoint buffers
+        out = [w() for w in work] if serial else concurrently(lambda w: w(), work)
+        phase_s["time_loop"] += t1 - t0
+        phase_s["adjoint_and_gradient"] += time.perf_counter() - t1
+        return out
 
     def launches():
         return sum(s.timing()["kernel_launches"] for s in fast) + batch.launches()
 
-    fast_out = fast_pass(serial=True)
-    for _ in range(max(args.warmup - 1, 0)):
+    fast_pass(serial=True, cap=20)
+    for _ in range(max(args.warmup, 1)):
         fast_out = fast_pass()
     # the same pass without the network's guesses (untimed): what it saves
     cold_it = [o["iters"] for o in fast_pass(warm=False)] if ws else None
@@ -454,6 +461,8 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = launches()
+    for k in phase_s:
+        phase_s[k] = 0.0
     with Clocks(dev) as clk:
         torch.cuda.synchronize()
         e0.record(stream)
@@ -464,12 +473,13 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
     n_launch = launches() - l0
     barrier()
     fast_ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+    fast_phases = {k: round(1e3 * v / args.steps, 1) for k, v in phase_s.items()}
     value = replica_throughput(world, len(cands), fast_ms / 1e3)
     log(f"fast arm {fast_ms:.1f} ms per pass")
 
     # plain arm (the denominator): its own warm-up, then timed passes
-    for _ in range(args.plain_warmup):
-        plain_out = plain_pass()
+    for _ in range(args.plain_warmup):  # allocations and graphs (short adjoints)
+        plain_out = plain_pass(cap=20)
     torch.cuda.synchronize()
     barrier()
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -532,6 +542,7 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
             "plain": "FP64 residual (bit-exact), one context at a time, block-ILU(0) BiCGSTAB from zero "
                      "(sweeps chosen by size for a solve alone)",
             "plain_fp64_evals_per_s": plain_value, "plain_ms_per_step": plain_ms,
+            "fast_ms_per_step_by_phase": fast_phases,
             "fast_over_plain": value / plain_value,
             "dJ_rel_err_max": max(errs), "dJ_rel_err": errs, "dJ_bar": DJ_BAR, "dJ_bar_met": max(errs) <= DJ_BAR,
             "target_5x_met": value / plain_value >= 5.0 and max(errs) <= DJ_BAR,
@@ -713,9 +724,9 @@ def main() -> int:
     ap.add_argument("--impl", default="o2f", choices=["o2f", "reference"])
     ap.add_argument("--workload", default="candidates", choices=["candidates", "large", "kernels"])
     ap.add_argument("--mesh", default="large", choices=["large", "medium"], help="mesh of --workload kernels")
-    ap.add_argument("--candidates", type=int, default=16)
+    ap.add_argument("--candidates", type=int, default=32)
     ap.add_argument("--cells-lo", type=float, default=30_000)
-    ap.add_argument("--cells-hi", type=float, default=120_000)
+    ap.add_argument("--cells-hi", type=float, default=80_000)
     ap.add_argument("--first-height", type=float, default=1e-3)
     ap.add_argument("--rk-steps", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=2024)

@@ -453,10 +453,13 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
         return sum(s.timing()["kernel_launches"] for s in fast) + batch.launches()
 
     fast_pass(serial=True, cap=20)
-    for _ in range(max(args.warmup, 1)):
-        fast_out = fast_pass()
-    # the same pass without the network's guesses (untimed): what it saves
-    cold_it = [o["iters"] for o in fast_pass(warm=False)] if ws else None
+    # warm-up passes; the first without the network's guesses, to show what
+    # the warm start saves
+    cold_it = None
+    for k in range(max(args.warmup, 1)):
+        fast_out = fast_pass(warm=k > 0 or ws is None)
+        if k == 0 and ws is not None:
+            cold_it = [o["iters"] for o in fast_out]
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -1360,6 +1360,9 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
     adjoint_rhs(beta, nullptr);
   }
   const int64_t nc = topo_.nc, n4 = 4 * nc;
+  // Grid of the Krylov vector kernels: one cell per thread up to the fixed
+  // reduction grid, so a small solve leaves the rest of the GPU to others.
+  const int kgrid = (int)std::min<int64_t>(kRedGrid, std::max<int64_t>(1, (nc + kBlock - 1) / kBlock));
   auto need = [&](Vec4<double>*& p) {
     if (!p) p = arena_.alloc<Vec4<double>>(nc);
   };
@@ -1377,7 +1380,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   else
     O2F_CUDA(cudaMemsetAsync(lam_, 0, nc * sizeof(Vec4<double>), stream_));
   // ||b||^2
-  k_dot2<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_), reinterpret_cast<double*>(b_), nullptr,
+  k_dot2<<<kgrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_), reinterpret_cast<double*>(b_), nullptr,
                                            nullptr, part_, ticket_, scal_);
   double bb[2];
   O2F_CUDA(cudaMemcpyAsync(bb, scal_, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -1412,29 +1415,29 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
   cudaGraphExec_t exec;
   O2F_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
   for (int i = 0; i < kItersPerGraph; ++i) {
-    k_bicg_p<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_),
+    k_bicg_p<<<kgrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_),
                                                reinterpret_cast<double*>(p_), reinterpret_cast<double*>(v_), ks_);
     if (precond) ilu_apply(p_, ph, kgate);
     if (full)
-      k_bicg_fjt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, ph, v_, r0_, part_, ks_);
+      k_bicg_fjt_v<<<kgrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, ph, v_, r0_, part_, ks_);
     else if (mixed_adjoint())  // FP32 blocks; restarts take the true residual with the FP64 operator
-      k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, ph, v_, r0_,
+      k_bicg_jt_v<<<kgrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, ph, v_, r0_,
                                                     part_, ks_);
     else
-      k_bicg_jt_v<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ph, v_, r0_,
+      k_bicg_jt_v<<<kgrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, ph, v_, r0_,
                                                     part_, ks_);
-    k_bicg_s<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(v_),
+    k_bicg_s<<<kgrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(r_), reinterpret_cast<double*>(v_),
                                                reinterpret_cast<double*>(s_), ks_);
     if (precond) ilu_apply(s_, sh, kgate);
     if (full)
-      k_bicg_fjt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, sh, s_, t_, part_, ks_);
+      k_bicg_fjt_t<<<kgrid, kBlock, 0, stream_>>>(nc, fjac_off_, fjac_idx_, fjac_blk_, sh, s_, t_, part_, ks_);
     else if (mixed_adjoint())
-      k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, sh, s_, t_,
+      k_bicg_jt_t<<<kgrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk32_, sh, s_, t_,
                                                     part_, ks_);
     else
-      k_bicg_jt_t<<<kRedGrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, sh, s_, t_,
+      k_bicg_jt_t<<<kgrid, kBlock, 0, stream_>>>(nc, topo_.jslot, geom_, topo_.ec, topo_.ebc, blk_, sh, s_, t_,
                                                     part_, ks_);
-    k_bicg_xr<<<kRedGrid, kBlock, 0, stream_>>>(n4, x, reinterpret_cast<double*>(ph), reinterpret_cast<double*>(sh),
+    k_bicg_xr<<<kgrid, kBlock, 0, stream_>>>(n4, x, reinterpret_cast<double*>(ph), reinterpret_cast<double*>(sh),
                                                 reinterpret_cast<double*>(s_), reinterpret_cast<double*>(t_),
                                                 reinterpret_cast<double*>(r_), reinterpret_cast<double*>(r0_), part_,
                                                 ks_);
@@ -1454,7 +1457,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
         ks.it = total;
         O2F_CUDA(cudaMemcpyAsync(ks_, &ks, sizeof(KrylovState), cudaMemcpyHostToDevice, stream_));
         jt_apply_dev(lam_, tmp_);
-        k_bicg_start<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_),
+        k_bicg_start<<<kgrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_),
                                                        reinterpret_cast<double*>(tmp_), reinterpret_cast<double*>(r_),
                                                        reinterpret_cast<double*>(r0_), reinterpret_cast<double*>(p_),
                                                        reinterpret_cast<double*>(v_), part_, ks_);
@@ -1473,7 +1476,7 @@ void Solver::adjoint_solve(double beta, double tol, int64_t max_iter, int64_t re
         total += chunk_its;
         // True residual (src/shape_optimization.cpp:716-717).
         jt_apply_dev(lam_, tmp_);
-        k_bicg_start<<<kRedGrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_),
+        k_bicg_start<<<kgrid, kBlock, 0, stream_>>>(n4, reinterpret_cast<double*>(b_),
                                                        reinterpret_cast<double*>(tmp_), reinterpret_cast<double*>(s_),
                                                        reinterpret_cast<double*>(t_), reinterpret_cast<double*>(p_),
                                                        reinterpret_cast<double*>(v_), part_, ks_);

@@ -359,9 +359,20 @@ class WarmStart:
         log(f"warm start: {self.n_fields} fields, {self.n_points} points, {train_steps} Adam steps in "
             f"{self.train_s:.1f} s, loss {self.final_loss:.4f}")
 
-    def guess(self, s, c: Candidate) -> np.ndarray:
-        return self.ws.adjoint_guess(self.net, self.norm, s, c.spec.m, c.spec.p, c.spec.t, beta=BETA,
+    def guess(self, s, c: Candidate):
+        """The network's lambda scaled by the alpha that minimises
+        ||b - J^T alpha lambda0|| (one J^T product), or None -- start from
+        zero -- when even that leaves more than 90 % of ||b||: a poor guess
+        can cost BiCGSTAB more iterations than it saves."""
+        lam0 = self.ws.adjoint_guess(self.net, self.norm, s, c.spec.m, c.spec.p, c.spec.t, beta=BETA,
                                      scaler=self.scaler)
+        b = s.assemble_adjoint_rhs(BETA)
+        a0 = s.apply_jacobian_transpose(lam0)
+        aa, ab, bb = float(a0 @ a0), float(a0 @ b), float(b @ b)
+        if aa <= 0.0 or bb <= 0.0:
+            return None
+        left = 1.0 - ab * ab / (aa * bb)  # ||b - alpha a0||^2 / ||b||^2 at the best alpha
+        return (ab / aa) * lam0 if left < 0.81 else None
 
 
 def concurrently(fn, items) -> list:

@@ -65,10 +65,11 @@ ADJ_TOL = 1e-8
 BETA = 0.1
 NAMES = ["m", "p", "t"]
 
-# DRAM bytes per launch of k_cell_gradient (FP64) per cell, from an ncu
-# capture of the current kernel (profiles/); scaled by cells to the 2.0M
-# mesh.  None until a capture of the current kernel exists.
-TRAFFIC_PER_CELL = {"cell_gradient": None}
+# DRAM bytes per launch of k_cell_gradient (FP64) per cell: dram__bytes_read
+# + dram__bytes_write of one ncu capture on the 1,014,040-cell mesh
+# (profiles/k_cell_gradient_fp64_1M.md, 329,626,368 B), scaled by cells to
+# the 2.0M mesh.
+TRAFFIC_PER_CELL = {"cell_gradient": 329_626_368 / 1_014_040}
 
 
 def naca_name(spec) -> str:

@@ -467,11 +467,38 @@ __device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, c
   if (!kForward) z[i] = v;
 }
 
+// Bulk prefetch of [p, p + bytes) into L2 (a hint: no data is returned and
+// no completion is awaited); p 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The L2 prefetch of one level [b, e) of a block sweep, by one warp: the
+// 32-position chunks of packed factor blocks that hold it (16 KiB each, plus
+// 4 KiB of D^-1 backward) and its records (32 B per position).  The chunks
+// lie inside the packed copy (n rounded up to 32 positions), the records
+// inside the 2n records of the two directions.
+template <bool kForward>
+__device__ __forceinline__ void sweep_prefetch_level(const IluDev& ilu, const int* rec, int b, int e, int lane) {
+  if (b >= e) return;
+  const int64_t n32 = ((int64_t)ilu.nc + 31) / 32 * 32;
+  for (int c = (b >> 5) + lane; c <= ((e - 1) >> 5); c += 32) {
+    prefetch_l2_bulk(ilu.pack + (kForward ? 0 : n32 * 64) + (int64_t)c * 2048, 2048 * sizeof(double));
+    if (!kForward) prefetch_l2_bulk(ilu.pack + 2 * n32 * 64 + (int64_t)c * 512, 512 * sizeof(double));
+  }
+  const char* r0 = reinterpret_cast<const char*>(rec + 8 * (int64_t)b);
+  const int64_t bytes = (int64_t)(e - b) * 8 * sizeof(int);
+  for (int64_t o = (int64_t)lane * 4096; o < bytes; o += 32 * 4096)
+    prefetch_l2_bulk(r0 + o, (uint32_t)(bytes - o < 4096 ? bytes - o : 4096));
+}
+
 // The first two rows of each thread in a level are software-pipelined: their
 // records are loaded during the level before and their own values (r, or the
 // forward value) requested at its end, so a level starts with its operands
 // in flight; further rows load at use.  Factor blocks come from the packed
-// copy (k_ilu_pack), coalesced across the warp.
+// copy (k_ilu_pack), coalesced across the warp; the first warp requests the
+// blocks and records of the level two ahead into L2 as each level starts,
+// for when other contexts' sweeps and products have evicted them.
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
                                                                     Vec4<double>* z, const int* gate) {
@@ -487,6 +514,8 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
   auto own_of = [&](const int4& a, const int4& c) { return kForward ? r[a.x] : ilu.out_f[c.z]; };
   int4 ra[2], rc[2];
   Vec4<double> own[2];
+  if (t < 32)
+    for (int l = 0; l < 2 && l < nlev; ++l) sweep_prefetch_level<kForward>(ilu, rec, off[l], off[l + 1], t);
   if (nlev > 0)
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
@@ -500,6 +529,7 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
   for (int l = 0; l < nlev; ++l) {
     const int b = off[l], e = off[l + 1];
     const int ne = l + 1 < nlev ? off[l + 2] : e;
+    if (t < 32 && l + 2 < nlev) sweep_prefetch_level<kForward>(ilu, rec, ne, off[l + 3], t);
     int4 na[2], nc[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {  // the next level's records, in flight during this one

@@ -156,106 +156,13 @@ def select_fields(targets: Sequence[np.ndarray], factor: float = 10.0) -> list[i
     return [i for i, v in enumerate(peaks) if v <= factor * ref]
 
 
-def wall_disc_coords(ctr: np.ndarray, seg_a: np.ndarray, seg_b: np.ndarray, h_rel: float = 1e-3,
-                     far: float = 20.0) -> np.ndarray:
-    """[n, 2] body-fitted coordinates of the points `ctr` [n, 2] about a wall
-    given as segments seg_a -> seg_b ([m, 2] end points, chained head to
-    tail into closed loops): the nearest wall point's arc-length fraction s
-    (from the rightmost wall point of its loop) and the wall distance d,
-    mapped to the disc rho (cos 2 pi s, sin 2 pi s) with
-    rho = 1 + log(1 + d/h) / log(1 + far/h) and h = h_rel x chord (the
-    wall's x extent).  The wall maps to the unit circle and the far field to
-    about radius 2, the boundary layer (d ~ h to 100 h) to rho in
-    [1.07, 1.5]: the fields the network learns vary over the disc at one
-    scale instead of at 1e-3 and at 20 chords in (x, y)."""
-    from scipy.spatial import cKDTree
-    ctr = np.asarray(ctr, dtype=np.float64).reshape(-1, 2)
-    a = np.asarray(seg_a, dtype=np.float64).reshape(-1, 2)
-    b = np.asarray(seg_b, dtype=np.float64).reshape(-1, 2)
-    m = a.shape[0]
-    # chain the segments into loops by shared end points; arc length per loop
-    key = lambda p: (round(p[0], 12), round(p[1], 12))
-    starts = {}
-    for k in range(m):
-        starts.setdefault(key(a[k]), []).append(k)
-    s0 = np.zeros(m)
-    total = np.ones(m)
-    seen = np.zeros(m, dtype=bool)
-    seglen = np.hypot(*(b - a).T)
-    for first in np.argsort(-a[:, 0], kind="stable"):  # a loop starts at its rightmost point
-        if seen[first]:
-            continue
-        loop, k = [], int(first)
-        while k is not None and not seen[k]:
-            seen[k] = True
-            loop.append(k)
-            nxt = [j for j in starts.get(key(b[k]), []) if not seen[j]]
-            k = nxt[0] if nxt else None
-        cum = np.concatenate([[0.0], np.cumsum(seglen[loop])])
-        s0[loop], total[loop] = cum[:-1], max(cum[-1], 1e-300)
-    xs = np.concatenate([a[:, 0], b[:, 0]])
-    h = h_rel * max(float(xs.max() - xs.min()), 1e-300)
-    kq = min(8, m)
-    _, idx = cKDTree(0.5 * (a + b)).query(ctr, k=kq)
-    idx = idx.reshape(ctr.shape[0], kq)
-    ab = b[idx] - a[idx]  # [n, k, 2]
-    ap = ctr[:, None, :] - a[idx]
-    t = np.clip(np.sum(ap * ab, axis=2) / np.maximum(np.sum(ab * ab, axis=2), 1e-300), 0.0, 1.0)
-    q = a[idx] + t[..., None] * ab
-    d2 = np.sum((ctr[:, None, :] - q) ** 2, axis=2)
-    j = np.argmin(d2, axis=1)
-    r = np.arange(ctr.shape[0])
-    seg = idx[r, j]
-    d = np.sqrt(d2[r, j])
-    s = (s0[seg] + t[r, j] * seglen[seg]) / total[seg]
-    rho = 1.0 + np.log1p(d / h) / np.log1p(far / h)
-    ang = 2.0 * np.pi * s
-    return np.stack([rho * np.cos(ang), rho * np.sin(ang)], axis=1)
-
-
-def wall_segments(solver) -> tuple[np.ndarray, np.ndarray]:
-    """End points ([m, 2] each) of a context's wall edges, oriented so that
-    the segments chain into loops (each segment's end starts the next one)."""
-    xy = solver.mesh_array("vert_xy").reshape(-1, 2)
-    ev = solver.mesh_array("edge_v").reshape(-1, 2)
-    wall = ev[solver.mesh_array("edge_bc") == ord("w")]
-    adj = {}
-    for k, (u, v) in enumerate(wall):
-        adj.setdefault(int(u), []).append(k)
-        adj.setdefault(int(v), []).append(k)
-    used = np.zeros(len(wall), dtype=bool)
-    A, B = [], []
-    for k0 in range(len(wall)):
-        if used[k0]:
-            continue
-        u, v = int(wall[k0][0]), int(wall[k0][1])
-        k = k0
-        while True:
-            used[k] = True
-            A.append(u)
-            B.append(v)
-            nxt = [j for j in adj[v] if not used[j]]
-            if not nxt:
-                break
-            k = nxt[0]
-            u, v = v, int(wall[k][1]) if int(wall[k][0]) == v else int(wall[k][0])
-    return xy[np.array(A, dtype=np.int64)], xy[np.array(B, dtype=np.int64)]
-
-
-def cell_inputs(solver, m: float, p: float, t: float, coords: str = "xy") -> np.ndarray:
+def cell_inputs(solver, m: float, p: float, t: float) -> np.ndarray:
     """[n_cells, 7] network inputs of a context: cell centres (reference
-    order) -- as (x, y), or with coords="wall" as the body-fitted disc
-    coordinates of wall_disc_coords -- with the shape and the flow (Mach,
-    AoA) of its parameters."""
+    order) with the shape and the flow (Mach, AoA) of its parameters."""
     ctr = solver.mesh_array("cell_ctr").reshape(-1, 2)
     n = ctr.shape[0]
     x = np.empty((n, N_IN), dtype=np.float32)
-    if coords == "wall":
-        x[:, 0:2] = wall_disc_coords(ctr, *wall_segments(solver))
-    elif coords == "xy":
-        x[:, 0:2] = ctr
-    else:
-        raise ValueError(f"coords must be 'xy' or 'wall', not {coords!r}")
+    x[:, 0:2] = ctr
     x[:, 2], x[:, 3], x[:, 4] = m, p, t
     x[:, 5] = solver.params.inflow_velocity
     x[:, 6] = solver.params.aoa_deg
@@ -270,8 +177,7 @@ def _size(solver) -> np.ndarray:
     return np.sqrt(solver.mesh_array("cell_vol")).reshape(-1, 1)
 
 
-def sample(solver, m: float, p: float, t: float, steps: int, beta: float = 0.1, tol: float = 1e-10,
-           coords: str = "xy"):
+def sample(solver, m: float, p: float, t: float, steps: int, beta: float = 0.1, tol: float = 1e-10):
     """One training sample set: march `steps` RK3 steps from the freestream,
     solve the adjoint, return (inputs, targets [state, lambda/sqrt(V)] per
     cell)."""
@@ -279,21 +185,19 @@ def sample(solver, m: float, p: float, t: float, steps: int, beta: float = 0.1, 
     solver.time_loop(steps)
     U = solver.get_state().reshape(-1, 4)
     lam = solver.solve_adjoint_system(beta=beta, tol=tol)["lambda"].reshape(-1, 4)
-    return cell_inputs(solver, m, p, t, coords), np.concatenate([U, lam / _size(solver)], axis=1)
+    return cell_inputs(solver, m, p, t), np.concatenate([U, lam / _size(solver)], axis=1)
 
 
 def adjoint_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t: float,
-                  beta: float = 0.1, residual_scaled: bool = False, scaler: InputScaler | None = None,
-                  coords: str = "xy") -> np.ndarray:
+                  beta: float = 0.1, residual_scaled: bool = False, scaler: InputScaler | None = None) -> np.ndarray:
     """Predicted lambda (reference order, interleaved 4 per cell).  With
     residual_scaled, it is multiplied by the alpha minimising
     ||b - J^T (alpha lambda0)|| (one J^T product), which bounds the initial
     residual by ||b||; J^T weighs the guess's cell-scale error by 1/h, so
     that alpha can vanish for a guess that is close in L2.  Needs the
     interface states of the current state.  `scaler`: the input
-    standardisation the network was trained with; `coords`: its input
-    coordinates (cell_inputs)."""
-    x = cell_inputs(solver, m, p, t, coords)
+    standardisation the network was trained with."""
+    x = cell_inputs(solver, m, p, t)
     y = norm.from_net(net.predict(scaler.apply(x) if scaler else x))
     lam0 = np.ascontiguousarray((y[:, 4:8] * _size(solver)).reshape(-1))
     if not residual_scaled:
@@ -306,7 +210,7 @@ def adjoint_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t:
 
 
 def state_guess(net: Network, norm: Normaliser, solver, m: float, p: float, t: float,
-                scaler: InputScaler | None = None, coords: str = "xy") -> np.ndarray:
-    x = cell_inputs(solver, m, p, t, coords)
+                scaler: InputScaler | None = None) -> np.ndarray:
+    x = cell_inputs(solver, m, p, t)
     y = norm.from_net(net.predict(scaler.apply(x) if scaler else x))
     return np.ascontiguousarray(y[:, 0:4].reshape(-1))

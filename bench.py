@@ -17,9 +17,11 @@ gradient dJ/d(m, p, t) from the perturbed-residual pairs.
              CUDA graph; FP64 residual by default, --fast-precision fp32 for
              the FP32 residual accumulated into the FP64 state), then every
              candidate's adjoint at once, each context on its own stream:
-             BiCGSTAB started from the warm-start network's prediction, with
-             FP32 J^T products and FP64 iterative refinement (true residual
-             in FP64), FP64 forces, J and gradient.
+             BiCGSTAB started from the warm-start network's prediction
+             (scaled to the least initial residual; from zero when that
+             leaves more than 81 % of ||b||^2 -- the line reports how many
+             guesses were used), with FP32 J^T products and FP64 iterative
+             refinement (true residual in FP64), FP64 forces, J and gradient.
 
 A "step" is one pass of the fast arm over every candidate.  `value` is fast
 evaluations per second, device time (CUDA events) with the meshes resident;
@@ -357,6 +359,7 @@ class WarmStart:
         self.train_s = time.perf_counter() - t0
         self.n_fields, self.n_points = len(keep), int(X.shape[0])
         self.final_loss = float(np.mean(hist[-50:]))
+        self.left = []  # residual fractions of the guesses of the last pass
         log(f"warm start: {self.n_fields} fields, {self.n_points} points, {train_steps} Adam steps in "
             f"{self.train_s:.1f} s, loss {self.final_loss:.4f}")
 
@@ -371,8 +374,10 @@ class WarmStart:
         a0 = s.apply_jacobian_transpose(lam0)
         aa, ab, bb = float(a0 @ a0), float(a0 @ b), float(b @ b)
         if aa <= 0.0 or bb <= 0.0:
+            self.left.append(1.0)
             return None
         left = 1.0 - ab * ab / (aa * bb)  # ||b - alpha a0||^2 / ||b||^2 at the best alpha
+        self.left.append(left)
         return (ab / aa) * lam0 if left < 0.81 else None
 
 
@@ -453,6 +458,8 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
             raise RuntimeError(f"fast time loop failed for candidates {bad}")
         # the network's predictions (one network: one call at a time), then
         # every candidate's adjoint and gradient at once
+        if ws:
+            ws.left = []
         guesses = [ws.guess(s, c) if ws and warm else None for s, c in zip(fast, cands)]
         work = [lambda k=k: adjoint_and_gradient(fast[k], cands[k], guesses[k], cap) for k in range(len(cands))]
         # serial: a first, short pass allocates each context's adjoint buffers
@@ -568,7 +575,14 @@ def run_candidates(args, rank: int, world: int) -> dict | None:
                                                     "fields": ws.n_fields, "points": ws.n_points,
                                                     "adam_steps": args.train_steps,
                                                     "train_s": round(ws.train_s, 2),
-                                                    "loss": round(ws.final_loss, 5)},
+                                                    "loss": round(ws.final_loss, 5),
+                                                    "guesses_used": int(sum(v < 0.81 for v in ws.left)),
+                                                    "residual_left_min": round(min(ws.left), 5) if ws.left else None,
+                                                    "residual_left_median": round(float(np.median(ws.left)), 5)
+                                                    if ws.left else None,
+                                                    "rule": "guess alpha*lambda0 (alpha minimising ||b - J^T alpha "
+                                                            "lambda0||) used when it leaves < 0.81 of ||b||^2, "
+                                                            "else a cold start"},
             "l2": "inputs larger than L2 (working set of the batch > 126 MB)",
             "parallelism": f"replicas x{world}"},
         "clocks": clk.summary(),

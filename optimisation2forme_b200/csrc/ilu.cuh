@@ -390,7 +390,16 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
 // many contexts run side by side.
 constexpr int kSweepCtaThreads = 512;
 constexpr int kSweepWindow = 4096;  // values kept in shared memory (128 KiB)
-constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow;
+// Factor blocks of the next level staged in shared memory (two buffers,
+// alternating by level): the first 3 chunks of 32 positions forward (16 KiB
+// each), the first 2 backward with their D^-1 (4 KiB each) after them.
+constexpr int kStageChunksFwd = 3;
+constexpr int kStageChunksBwd = 2;
+constexpr int kStageBwdD = kStageChunksBwd * 2048;  // offset of the staged D^-1, doubles
+constexpr int kStageDoubles = kStageChunksFwd * 2048;  // one buffer (backward uses 2*2048 + 2*512)
+constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow + 2 * kStageDoubles * sizeof(double);
+static_assert(kSweepSmem <= 227 * 1024, "block sweep shared memory above the per-block limit");
+static_assert(kStageBwdD + kStageChunksBwd * 512 <= kStageDoubles, "backward staging overflows its buffer");
 
 // Factor blocks of the block sweeps, repacked in sweep order after every
 // factorization and interleaved over 32 consecutive positions, so that the
@@ -429,15 +438,20 @@ __global__ void k_ilu_pack(int n, IluDev ilu) {
 
 // One row of a block sweep: own value minus the dependencies' products
 // (slot order), times D^-1 backward; stored in the window, by position, and
-// (backward) into z by row.
+// (backward) into z by row.  Factor blocks of the level's first `nch` chunks
+// (from chunk c0) are read from the staged copy `stage`, the rest from the
+// packed copy in global memory: same layout, same values.
 template <bool kForward>
 __device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, const int4& a, const int4& c,
                                               Vec4<double> acc, const Vec4<double>* win_r, Vec4<double>* win,
-                                              Vec4<double>* out, Vec4<double>* z) {
+                                              Vec4<double>* out, Vec4<double>* z, const double* stage, int c0,
+                                              int nch) {
   const int i = a.x;
   const int dq[4] = {a.y, a.z, a.w, c.x};
   const int64_t n32 = ((int64_t)ilu.nc + 31) / 32 * 32;
-  const double* P = ilu.pack + sweep_pack_base(n32, kForward ? 0 : 1, p);
+  const int k = (p >> 5) - c0;  // >= 0: p lies in the level that starts in chunk c0
+  const bool staged = k < nch;
+  const double* P = staged ? stage + k * 2048 + (p & 31) : ilu.pack + sweep_pack_base(n32, kForward ? 0 : 1, p);
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
     const int q = dq[d];
@@ -450,7 +464,8 @@ __device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, c
     acc.d -= Bk[384] * v.a + Bk[416] * v.b + Bk[448] * v.c + Bk[480] * v.d;
   }
   if (!kForward) {
-    const double* D = ilu.pack + 2 * n32 * 64 + (int64_t)(p >> 5) * 512 + (p & 31);
+    const double* D = staged ? stage + kStageBwdD + k * 512 + (p & 31)
+                             : ilu.pack + 2 * n32 * 64 + (int64_t)(p >> 5) * 512 + (p & 31);
     Vec4<double> o4;
     o4.a = D[0] * acc.a + D[32] * acc.b + D[64] * acc.c + D[96] * acc.d;
     o4.b = D[128] * acc.a + D[160] * acc.b + D[192] * acc.c + D[224] * acc.d;
@@ -492,13 +507,48 @@ __device__ __forceinline__ void sweep_prefetch_level(const IluDev& ilu, const in
     prefetch_l2_bulk(r0 + o, (uint32_t)(bytes - o < 4096 ? bytes - o : 4096));
 }
 
+// Asynchronous 16-byte global -> shared copy (completes at cp_async_wait_all).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Chunks of 32 positions of the level [b, e) that are staged.
+template <bool kForward>
+__device__ __forceinline__ int sweep_stage_chunks(int b, int e) {
+  if (b >= e) return 0;
+  const int n = ((e - 1) >> 5) - (b >> 5) + 1;
+  const int cap = kForward ? kStageChunksFwd : kStageChunksBwd;
+  return n < cap ? n : cap;
+}
+
+// Stage the factor blocks of level [b, e) into `buf`, by the whole block:
+// each copied chunk lies inside the packed copy (chunk indices up to
+// (e - 1) >> 5 < n32 / 32); addresses and sizes are multiples of 16 bytes.
+template <bool kForward>
+__device__ __forceinline__ void sweep_stage_level(const IluDev& ilu, int b, int e, double* buf, int t, int T) {
+  const int nch = sweep_stage_chunks<kForward>(b, e);
+  if (nch == 0) return;
+  const int64_t n32 = ((int64_t)ilu.nc + 31) / 32 * 32;
+  const double* src = ilu.pack + (kForward ? 0 : n32 * 64) + (int64_t)(b >> 5) * 2048;
+  for (int k = t; k < nch * 1024; k += T) cp_async16(buf + 2 * k, src + 2 * k);
+  if (!kForward) {
+    const double* srcD = ilu.pack + 2 * n32 * 64 + (int64_t)(b >> 5) * 512;
+    for (int k = t; k < nch * 256; k += T) cp_async16(buf + kStageBwdD + 2 * k, srcD + 2 * k);
+  }
+}
+
 // The first two rows of each thread in a level are software-pipelined: their
 // records are loaded during the level before and their own values (r, or the
 // forward value) requested at its end, so a level starts with its operands
 // in flight; further rows load at use.  Factor blocks come from the packed
-// copy (k_ilu_pack), coalesced across the warp; the first warp requests the
-// blocks and records of the level two ahead into L2 as each level starts,
-// for when other contexts' sweeps and products have evicted them.
+// copy (k_ilu_pack), coalesced across the warp: the first chunks of each
+// level staged in shared memory by asynchronous copies issued during the
+// level before (two buffers), the rest read from global memory.  The first
+// warp also requests the blocks and records of the level two ahead into L2
+// as each level starts, for when other contexts' sweeps and products have
+// evicted them.
 template <bool kForward>
 __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
                                                                     Vec4<double>* z, const int* gate) {
@@ -512,11 +562,13 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
   auto rec_a = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p); };
   auto rec_c = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p + 4); };
   auto own_of = [&](const int4& a, const int4& c) { return kForward ? r[a.x] : ilu.out_f[c.z]; };
+  double* stg = reinterpret_cast<double*>(win + kSweepWindow);  // 2 x kStageDoubles
   int4 ra[2], rc[2];
   Vec4<double> own[2];
   if (t < 32)
     for (int l = 0; l < 2 && l < nlev; ++l) sweep_prefetch_level<kForward>(ilu, rec, off[l], off[l + 1], t);
-  if (nlev > 0)
+  if (nlev > 0) {
+    sweep_stage_level<kForward>(ilu, off[0], off[1], stg, t, T);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int p = off[0] + t + k * T;
@@ -526,10 +578,18 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
         own[k] = own_of(ra[k], rc[k]);
       }
     }
+    cp_async_wait_all();
+    __syncthreads();
+  }
   for (int l = 0; l < nlev; ++l) {
     const int b = off[l], e = off[l + 1];
     const int ne = l + 1 < nlev ? off[l + 2] : e;
     if (t < 32 && l + 2 < nlev) sweep_prefetch_level<kForward>(ilu, rec, ne, off[l + 3], t);
+    // this level's staged blocks (filled during the level before); the next
+    // level's into the other buffer, whose last readers passed the barrier
+    const double* cur = stg + (l & 1) * kStageDoubles;
+    const int c0 = b >> 5, nch = sweep_stage_chunks<kForward>(b, e);
+    if (l + 1 < nlev) sweep_stage_level<kForward>(ilu, e, ne, stg + ((l + 1) & 1) * kStageDoubles, t, T);
     int4 na[2], nc[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {  // the next level's records, in flight during this one
@@ -542,11 +602,11 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int p = b + t + k * T;
-      if (p < e) sweep_cta_row<kForward>(ilu, p, e, ra[k], rc[k], own[k], win, win, out, z);
+      if (p < e) sweep_cta_row<kForward>(ilu, p, e, ra[k], rc[k], own[k], win, win, out, z, cur, c0, nch);
     }
     for (int p = b + t + 2 * T; p < e; p += T) {
       const int4 a = rec_a(p), c = rec_c(p);
-      sweep_cta_row<kForward>(ilu, p, e, a, c, own_of(a, c), win, win, out, z);
+      sweep_cta_row<kForward>(ilu, p, e, a, c, own_of(a, c), win, win, out, z, cur, c0, nch);
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {  // the next level's operands, requested before the barrier
@@ -557,6 +617,7 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
         own[k] = own_of(ra[k], rc[k]);
       }
     }
+    cp_async_wait_all();  // this thread's copies of the next level, visible to all after the barrier
     __syncthreads();
   }
 }

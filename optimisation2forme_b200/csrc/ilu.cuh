@@ -389,14 +389,14 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
 // k_ilu_sweep: both give the same bits.  One SM per sweep, so the sweeps of
 // many contexts run side by side.
 constexpr int kSweepCtaThreads = 512;
-constexpr int kSweepWindow = 4096;  // values kept in shared memory (128 KiB)
+constexpr int kSweepWindow = 2048;  // values kept in shared memory (64 KiB; ~96 % of the dependencies)
 // Factor blocks of the next level staged in shared memory (two buffers,
-// alternating by level): the first 3 chunks of 32 positions forward (16 KiB
-// each), the first 2 backward with their D^-1 (4 KiB each) after them.
-constexpr int kStageChunksFwd = 3;
-constexpr int kStageChunksBwd = 2;
+// alternating by level): the first 5 chunks of 32 positions forward (16 KiB
+// each), the first 4 backward with their D^-1 (4 KiB each) after them.
+constexpr int kStageChunksFwd = 5;
+constexpr int kStageChunksBwd = 4;
 constexpr int kStageBwdD = kStageChunksBwd * 2048;  // offset of the staged D^-1, doubles
-constexpr int kStageDoubles = kStageChunksFwd * 2048;  // one buffer (backward uses 2*2048 + 2*512)
+constexpr int kStageDoubles = kStageChunksFwd * 2048;  // one buffer (backward uses 4*2048 + 4*512)
 constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow + 2 * kStageDoubles * sizeof(double);
 static_assert(kSweepSmem <= 227 * 1024, "block sweep shared memory above the per-block limit");
 static_assert(kStageBwdD + kStageChunksBwd * 512 <= kStageDoubles, "backward staging overflows its buffer");

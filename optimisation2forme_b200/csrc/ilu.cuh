@@ -539,19 +539,19 @@ __device__ __forceinline__ void sweep_stage_level(const IluDev& ilu, int b, int 
   }
 }
 
-// The first row of each thread in a level is software-pipelined: its record
-// is loaded two levels ahead and its own value (r, or the forward value;
-// neither depends on this sweep) requested as the level before starts, so
-// both loads have a whole level to arrive; further rows (levels wider than
-// the block) load at use.  Factor blocks come from the packed copy
-// (k_ilu_pack), coalesced across the warp: the first chunks of each level
-// staged in shared memory by asynchronous copies issued during the level
-// before (two buffers), the rest read from global memory.  The first warp
-// also requests the blocks and records of the level two ahead into L2 as
-// each level starts, for when other contexts' sweeps and products have
-// evicted them.
+// The first two rows of each thread in a level are software-pipelined: their
+// records are loaded during the level before and their own values (r, or the
+// forward value) requested at its end, so a level starts with its operands
+// in flight; further rows load at use.  Factor blocks come from the packed
+// copy (k_ilu_pack), coalesced across the warp: the first chunks of each
+// level staged in shared memory by asynchronous copies issued during the
+// level before (two buffers), the rest read from global memory.  The first
+// warp also requests the blocks and records of the level two ahead into L2
+// as each level starts, for when other contexts' sweeps and products have
+// evicted them.  One block per SM is declared so that the compiler keeps the
+// rows' loads in registers (about 100 per thread) instead of capping them.
 template <bool kForward>
-__global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
+__global__ void __launch_bounds__(kSweepCtaThreads, 1) k_ilu_sweep_cta(int n, IluDev ilu, const Vec4<double>* r,
                                                                     Vec4<double>* z, const int* gate) {
   if (gated(gate)) return;
   extern __shared__ Vec4<double> win[];
@@ -563,25 +563,22 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
   auto rec_a = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p); };
   auto rec_c = [&](int p) { return *reinterpret_cast<const int4*>(rec + 8 * (int64_t)p + 4); };
   auto own_of = [&](const int4& a, const int4& c) { return kForward ? r[a.x] : ilu.out_f[c.z]; };
-  // does this thread have a first row in level L?
-  auto first = [&](int L) { return L < nlev && off[L] + t < off[L + 1]; };
   double* stg = reinterpret_cast<double*>(win + kSweepWindow);  // 2 x kStageDoubles
-  // this thread's first row of level l (a0, c0, own0), l + 1 (a1, c1, own1), l + 2 (a2, c2)
-  int4 a0{}, c0{}, a1{}, c1{}, a2{}, c2{};
-  Vec4<double> own0{}, own1{};
+  int4 ra[2], rc[2];
+  Vec4<double> own[2];
   if (t < 32)
     for (int l = 0; l < 2 && l < nlev; ++l) sweep_prefetch_level<kForward>(ilu, rec, off[l], off[l + 1], t);
   if (nlev > 0) {
     sweep_stage_level<kForward>(ilu, off[0], off[1], stg, t, T);
-    if (first(0)) {
-      a0 = rec_a(off[0] + t);
-      c0 = rec_c(off[0] + t);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int p = off[0] + t + k * T;
+      if (p < off[1]) {
+        ra[k] = rec_a(p);
+        rc[k] = rec_c(p);
+        own[k] = own_of(ra[k], rc[k]);
+      }
     }
-    if (first(1)) {
-      a1 = rec_a(off[1] + t);
-      c1 = rec_c(off[1] + t);
-    }
-    if (first(0)) own0 = own_of(a0, c0);
     cp_async_wait_all();
     __syncthreads();
   }
@@ -592,24 +589,35 @@ __global__ void __launch_bounds__(kSweepCtaThreads) k_ilu_sweep_cta(int n, IluDe
     // this level's staged blocks (filled during the level before); the next
     // level's into the other buffer, whose last readers passed the barrier
     const double* cur = stg + (l & 1) * kStageDoubles;
-    const int ch0 = b >> 5, nch = sweep_stage_chunks<kForward>(b, e);
+    const int c0 = b >> 5, nch = sweep_stage_chunks<kForward>(b, e);
     if (l + 1 < nlev) sweep_stage_level<kForward>(ilu, e, ne, stg + ((l + 1) & 1) * kStageDoubles, t, T);
-    // in flight during this level: the next level's own value, the records two levels ahead
-    if (first(l + 1)) own1 = own_of(a1, c1);
-    if (first(l + 2)) {
-      a2 = rec_a(off[l + 2] + t);
-      c2 = rec_c(off[l + 2] + t);
+    int4 na[2], nc[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {  // the next level's records, in flight during this one
+      const int q = e + t + k * T;
+      if (q < ne) {
+        na[k] = rec_a(q);
+        nc[k] = rec_c(q);
+      }
     }
-    if (b + t < e) sweep_cta_row<kForward>(ilu, b + t, e, a0, c0, own0, win, win, out, z, cur, ch0, nch);
-    for (int p = b + t + T; p < e; p += T) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int p = b + t + k * T;
+      if (p < e) sweep_cta_row<kForward>(ilu, p, e, ra[k], rc[k], own[k], win, win, out, z, cur, c0, nch);
+    }
+    for (int p = b + t + 2 * T; p < e; p += T) {
       const int4 a = rec_a(p), c = rec_c(p);
-      sweep_cta_row<kForward>(ilu, p, e, a, c, own_of(a, c), win, win, out, z, cur, ch0, nch);
+      sweep_cta_row<kForward>(ilu, p, e, a, c, own_of(a, c), win, win, out, z, cur, c0, nch);
     }
-    a0 = a1;
-    c0 = c1;
-    own0 = own1;
-    a1 = a2;
-    c1 = c2;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {  // the next level's operands, requested before the barrier
+      const int q = e + t + k * T;
+      if (q < ne) {
+        ra[k] = na[k];
+        rc[k] = nc[k];
+        own[k] = own_of(ra[k], rc[k]);
+      }
+    }
     cp_async_wait_all();  // this thread's copies of the next level, visible to all after the barrier
     __syncthreads();
   }

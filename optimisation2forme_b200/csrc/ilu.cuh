@@ -391,12 +391,16 @@ __global__ void __launch_bounds__(kSweepBlock) k_ilu_sweep(int n, IluDev ilu, co
 constexpr int kSweepCtaThreads = 512;
 constexpr int kSweepWindow = 2048;  // values kept in shared memory (64 KiB; ~96 % of the dependencies)
 // Factor blocks of the next level staged in shared memory (two buffers,
-// alternating by level): the first 5 chunks of 32 positions forward (16 KiB
-// each), the first 4 backward with their D^-1 (4 KiB each) after them.
-constexpr int kStageChunksFwd = 5;
-constexpr int kStageChunksBwd = 4;
-constexpr int kStageBwdD = kStageChunksBwd * 2048;  // offset of the staged D^-1, doubles
-constexpr int kStageDoubles = kStageChunksFwd * 2048;  // one buffer (backward uses 4*2048 + 4*512)
+// alternating by level): dependency slots 0 and 1 of each position (on
+// triangles a forward row has at most 2 dependencies, a backward row rarely
+// 3) for the first 10 chunks of 32 positions forward (8 KiB each), the first
+// 6 backward with their D^-1 (4 KiB each) after them.
+constexpr int kStageSlots = 2;
+constexpr int kStageChunkDoubles = kStageSlots * 512;
+constexpr int kStageChunksFwd = 10;
+constexpr int kStageChunksBwd = 6;
+constexpr int kStageBwdD = kStageChunksBwd * kStageChunkDoubles;  // offset of the staged D^-1, doubles
+constexpr int kStageDoubles = kStageChunksFwd * kStageChunkDoubles;  // one buffer (backward: 6*1024 + 6*512)
 constexpr size_t kSweepSmem = sizeof(Vec4<double>) * kSweepWindow + 2 * kStageDoubles * sizeof(double);
 static_assert(kSweepSmem <= 227 * 1024, "block sweep shared memory above the per-block limit");
 static_assert(kStageBwdD + kStageChunksBwd * 512 <= kStageDoubles, "backward staging overflows its buffer");
@@ -451,12 +455,13 @@ __device__ __forceinline__ void sweep_cta_row(const IluDev& ilu, int p, int e, c
   const int64_t n32 = ((int64_t)ilu.nc + 31) / 32 * 32;
   const int k = (p >> 5) - c0;  // >= 0: p lies in the level that starts in chunk c0
   const bool staged = k < nch;
-  const double* P = staged ? stage + k * 2048 + (p & 31) : ilu.pack + sweep_pack_base(n32, kForward ? 0 : 1, p);
+  const double* P = ilu.pack + sweep_pack_base(n32, kForward ? 0 : 1, p);
+  const double* S = stage + k * kStageChunkDoubles + (p & 31);
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
     const int q = dq[d];
     if (q < 0) break;
-    const double* Bk = P + d * 512;  // element k at Bk[32 k]
+    const double* Bk = (staged && d < kStageSlots ? S : P) + d * 512;  // element k at Bk[32 k]
     const Vec4<double> v = q >= e - kSweepWindow ? win_r[q % kSweepWindow] : out[q];
     acc.a -= Bk[0] * v.a + Bk[32] * v.b + Bk[64] * v.c + Bk[96] * v.d;
     acc.b -= Bk[128] * v.a + Bk[160] * v.b + Bk[192] * v.c + Bk[224] * v.d;
@@ -524,7 +529,9 @@ __device__ __forceinline__ int sweep_stage_chunks(int b, int e) {
 }
 
 // Stage the factor blocks of level [b, e) into `buf`, by the whole block:
-// each copied chunk lies inside the packed copy (chunk indices up to
+// dependency slots 0 .. kStageSlots-1 of the level's first chunks (the
+// leading kStageChunkDoubles of each 2048-double chunk), and D^-1 backward.
+// Each copied chunk lies inside the packed copy (chunk indices up to
 // (e - 1) >> 5 < n32 / 32); addresses and sizes are multiples of 16 bytes.
 template <bool kForward>
 __device__ __forceinline__ void sweep_stage_level(const IluDev& ilu, int b, int e, double* buf, int t, int T) {
@@ -532,7 +539,11 @@ __device__ __forceinline__ void sweep_stage_level(const IluDev& ilu, int b, int 
   if (nch == 0) return;
   const int64_t n32 = ((int64_t)ilu.nc + 31) / 32 * 32;
   const double* src = ilu.pack + (kForward ? 0 : n32 * 64) + (int64_t)(b >> 5) * 2048;
-  for (int k = t; k < nch * 1024; k += T) cp_async16(buf + 2 * k, src + 2 * k);
+  constexpr int kPieces = kStageChunkDoubles / 2;  // 16-byte pieces per staged chunk
+  for (int k = t; k < nch * kPieces; k += T) {
+    const int ch = k / kPieces, pc = k - ch * kPieces;
+    cp_async16(buf + ch * kStageChunkDoubles + 2 * pc, src + (int64_t)ch * 2048 + 2 * pc);
+  }
   if (!kForward) {
     const double* srcD = ilu.pack + 2 * n32 * 64 + (int64_t)(b >> 5) * 512;
     for (int k = t; k < nch * 256; k += T) cp_async16(buf + kStageBwdD + 2 * k, srcD + 2 * k);

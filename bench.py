@@ -69,8 +69,8 @@ NAMES = ["m", "p", "t"]
 
 # DRAM bytes per launch of k_cell_gradient (FP64) per cell: dram__bytes_read
 # + dram__bytes_write of one ncu capture on the 1,014,040-cell mesh
-# (profiles/k_cell_gradient_fp64_1M.md, 329,626,368 B), scaled by cells to
-# the 2.0M mesh.
+# (`--workload kernels --mesh medium`, 329,626,368 B), scaled by cells to the
+# 2.0M mesh.
 TRAFFIC_PER_CELL = {"cell_gradient": 329_626_368 / 1_014_040}
 
 

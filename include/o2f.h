@@ -99,7 +99,7 @@ typedef enum o2f_status {
  * block walks the dependency levels (one SM per sweep: best when several
  * contexts solve at once, and alone on small meshes); WAITING: persistent
  * warps on up to 64 SMs, each row waiting on its dependencies (best alone on
- * large meshes); AUTO: BLOCK up to 70,000 cells, else WAITING. */
+ * large meshes); AUTO: BLOCK up to 200,000 cells, else WAITING. */
 #define O2F_SWEEPS_AUTO 0
 #define O2F_SWEEPS_BLOCK 1
 #define O2F_SWEEPS_WAITING 2

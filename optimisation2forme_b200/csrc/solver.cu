@@ -763,9 +763,10 @@ void Solver::ilu_factor() {
 }
 
 // O2F_SWEEPS_AUTO: triangles up to this many rows are swept by one thread
-// block (measured on B200: faster alone up to ~40-70k rows, and side by side
-// with other contexts' solves at every size measured).
-constexpr int64_t kIluCtaMaxRows = 70000;
+// block (measured on B200 per adjoint iteration alone, block / waiting:
+// 3.9 / 5.2 ms at 75k rows, 6.9 / 8.1 at 151k, 13.1 / 11.8 at 301k; side by
+// side with other contexts' solves the block sweep is ahead at every size).
+constexpr int64_t kIluCtaMaxRows = 200000;
 
 // z = M^{-1} r = U^{-1} L^{-1} r: the forward sweep into ilu_.tmp, the
 // backward sweep into z; one launch per triangle, either one block walking
